@@ -1,0 +1,101 @@
+// Shared device definitions: the D3Q19 lattice, population storage codecs and
+// NaN-propagating min/max with JavaScript's Math.min / Math.max semantics.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+namespace aerosim {
+
+// D3Q19 velocity set and opposite table, src/solver/lbmConstants.ts:10-48
+// (same ordering: rest, 6 faces, 12 edges).
+__host__ __device__ constexpr int cx_of(int d) {
+  return (d == 1 || d == 7 || d == 9 || d == 11 || d == 13) ? 1
+       : (d == 2 || d == 8 || d == 10 || d == 12 || d == 14) ? -1 : 0;
+}
+__host__ __device__ constexpr int cy_of(int d) {
+  return (d == 3 || d == 7 || d == 10 || d == 15 || d == 17) ? 1
+       : (d == 4 || d == 8 || d == 9 || d == 16 || d == 18) ? -1 : 0;
+}
+__host__ __device__ constexpr int cz_of(int d) {
+  return (d == 5 || d == 11 || d == 14 || d == 15 || d == 18) ? 1
+       : (d == 6 || d == 12 || d == 13 || d == 16 || d == 17) ? -1 : 0;
+}
+__host__ __device__ constexpr int opp_of(int d) { return d == 0 ? 0 : ((d & 1) ? d + 1 : d - 1); }
+
+// Exact double weights 1/3, 1/18, 1/36 (LBM_WEIGHTS) ...
+__host__ __device__ constexpr double w64_of(int d) {
+  return d == 0 ? 1.0 / 3.0 : (d <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+// ... and the float copy promoted to double (LBM_WEIGHTS_F32), used by the
+// reference's collision and force integrator.
+__host__ __device__ constexpr double w32_of(int d) { return (double)(float)w64_of(d); }
+__host__ __device__ constexpr float wf_of(int d) { return (float)w64_of(d); }
+
+constexpr uint8_t CELL_FLUID = 0, CELL_SOLID = 1, CELL_BOUNDARY = 2;
+// Cell class byte used by the solver kernels: the low 2 bits are the reference
+// flag; CLS_NEAR marks a non-solid cell with at least one SOLID clamped pull source.
+constexpr uint8_t CLS_FLAG_MASK = 3, CLS_NEAR = 4;
+
+// Math.min / Math.max: NaN if either operand is NaN.
+__host__ __device__ inline double js_min(double a, double b) {
+  return (a != a || b != b) ? a + b : (a < b ? a : b);
+}
+__host__ __device__ inline double js_max(double a, double b) {
+  return (a != a || b != b) ? a + b : (a > b ? a : b);
+}
+
+// FP16 storage scale: (f - w) * 2^15 keeps the deviations of a near-equilibrium
+// flow inside half's normal range (6.1e-5 .. 65504) with its full 11-bit mantissa.
+constexpr float F16S_SCALE = 32768.0f;
+constexpr float F16S_INV_SCALE = 1.0f / 32768.0f;
+
+// Population storage codecs.  All four expose the same interface in terms of the
+// deviation h = f - w_d from the rest weight (the form the FP32 collision works in)
+// and of the full value f (the form the FP64 paths work in):
+//   h_of(raw, d), raw_of_h(h, d)  -- float deviation
+//   f_of(raw, d), raw_of_f(f, d)  -- double value
+// d is a loop index of fully unrolled loops, so w_d folds to a constant.
+struct StoreF32 {
+  using T = float;
+  __device__ __forceinline__ static float h_of(T v, int d) { return v - wf_of(d); }
+  __device__ __forceinline__ static T raw_of_h(float h, int d) { return wf_of(d) + h; }
+  __device__ __forceinline__ static double f_of(T v, int) { return (double)v; }
+  __device__ __forceinline__ static T raw_of_f(double f, int) { return (float)f; }
+};
+struct StoreF64 {
+  using T = double;
+  __device__ __forceinline__ static float h_of(T v, int d) { return (float)(v - w64_of(d)); }
+  __device__ __forceinline__ static T raw_of_h(float h, int d) { return w64_of(d) + (double)h; }
+  __device__ __forceinline__ static double f_of(T v, int) { return v; }
+  __device__ __forceinline__ static T raw_of_f(double f, int) { return f; }
+};
+struct StoreF16S {
+  using T = __half;
+  __device__ __forceinline__ static float h_of(T v, int) { return __half2float(v) * F16S_INV_SCALE; }
+  __device__ __forceinline__ static T raw_of_h(float h, int) { return __float2half_rn(h * F16S_SCALE); }
+  __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)h_of(v, d); }
+  __device__ __forceinline__ static T raw_of_f(double f, int d) { return raw_of_h((float)(f - (double)wf_of(d)), d); }
+};
+struct StoreBF16S {
+  using T = __nv_bfloat16;
+  __device__ __forceinline__ static float h_of(T v, int) { return __bfloat162float(v); }
+  __device__ __forceinline__ static T raw_of_h(float h, int) { return __float2bfloat16_rn(h); }
+  __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)h_of(v, d); }
+  __device__ __forceinline__ static T raw_of_f(double f, int d) { return raw_of_h((float)(f - (double)wf_of(d)), d); }
+};
+
+// Device-resident solver state shared across steps.  Slot [s & 1] belongs to step s.
+struct StepState {
+  unsigned long long rho_sum[2];   // fixed-point sum of post-boundary densities
+  unsigned int ticket[2];          // CTA completion counters (last-CTA finalisation)
+  int apply[2];                    // 1 if step s triggered the mean-density rescale
+  double corr[2];                  // 1 / meanRho of step s
+  double cumulative_rescale;       // product of applied corrections
+  long long rescale_count;
+  int nan_seen;                    // a non-finite density reached the rescale sum
+  int error;                       // kernel-reported error code (0 = none)
+};
+
+}  // namespace aerosim

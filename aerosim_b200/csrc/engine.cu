@@ -1,0 +1,672 @@
+// C-ABI layer of libaerosim.so: the LBMEngine / voxelizeMeshToLattice surface of the
+// reference (src/solver/lbmEngine.ts, src/geometry/voxelizer.ts) over the sm_100a
+// kernels.  Host code only; every device buffer is owned by the engine handle.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/aerosim.h"
+#include "common.cuh"
+#include "engine_internal.h"
+#include "lbm_kernels.cuh"
+
+using namespace aerosim;
+
+struct aerosim_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  aerosim_config cfg{};
+  bool have_grid = false;
+  DevGrid g;
+  double dx = 0, origin[3] = {0, 0, 0};
+  long long fluid_count = 0;
+  void* f[2] = {nullptr, nullptr};
+  int cur = 0;                 // f[cur] holds the latest populations (fSrc)
+  int f_prec = -1;
+  long long f_cells = 0, stride = 0;
+  float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
+  double* abl = nullptr;
+  double* sin_tab = nullptr;
+  int tab_ny = 0;
+  StepState* st = nullptr;
+  double* force_partials = nullptr;
+  unsigned int* force_ticket = nullptr;
+  double* force_out = nullptr;
+  long long force_blocks_cap = 0;
+  unsigned long long* stats_buf = nullptr;
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
+  long long step_index = 0;
+  double last_ms = 0;
+  long long last_launches = 0;
+};
+
+namespace {
+
+std::string g_create_error;
+
+int fail(aerosim_engine* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+#define CU(h, x)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (x);                                                                 \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? AEROSIM_ERR_NOMEM : AEROSIM_ERR_CUDA, \
+                  std::string(#x) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+
+void free_grid(DevGrid& g) {
+  cudaFree(g.flags); cudaFree(g.cls); cudaFree(g.bmap); cudaFree(g.bcells);
+  cudaFree(g.q); cudaFree(g.minq);
+  g = DevGrid();
+}
+
+void free_pops(aerosim_engine* h) {
+  cudaFree(h->f[0]); cudaFree(h->f[1]);
+  h->f[0] = h->f[1] = nullptr;
+  cudaFree(h->mux); cudaFree(h->muy); cudaFree(h->muz); cudaFree(h->mrho);
+  h->mux = h->muy = h->muz = h->mrho = nullptr;
+  h->f_prec = -1;
+  h->f_cells = 0;
+}
+
+int prev_slot(const aerosim_engine* h) { return (int)((h->step_index + 1) & 1); }
+
+int reset_state(aerosim_engine* h) {
+  StepState s{};
+  s.corr[0] = s.corr[1] = 1.0;
+  s.cumulative_rescale = 1.0;
+  CU(h, cudaMemcpyAsync(h->st, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  return AEROSIM_OK;
+}
+
+// resetEquilibrium + fresh rescale state, lbmCpuReference.ts:114-143.
+int do_reset(aerosim_engine* h) {
+  const DevGrid& g = h->g;
+  CU(h, launch_init(h->cfg.precision, h->f[0], h->f[1], g.cls, h->mux, h->muy, h->muz, h->mrho, h->abl,
+                    h->stride, g.nx, g.ny, g.nz, h->cfg.u_inlet_lattice, h->cfg.ground_no_slip, h->stream));
+  h->cur = 0;
+  h->step_index = 0;
+  int rc = reset_state(h);
+  if (rc) return rc;
+  CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
+// Allocates population and macro buffers for the current grid and precision.
+int ensure_pops(aerosim_engine* h, bool* reallocated) {
+  *reallocated = false;
+  const long long N = h->g.N;
+  if (h->f[0] && h->f_prec == h->cfg.precision && h->f_cells == N) return AEROSIM_OK;
+  free_pops(h);
+  const size_t eb = precision_bytes(h->cfg.precision);
+  const long long stride = (N + 63) / 64 * 64;  // 256-byte aligned direction planes (FP32)
+  CU(h, cudaMalloc(&h->f[0], 19 * (size_t)stride * eb));
+  CU(h, cudaMalloc(&h->f[1], 19 * (size_t)stride * eb));
+  CU(h, cudaMalloc(&h->mux, N * sizeof(float)));
+  CU(h, cudaMalloc(&h->muy, N * sizeof(float)));
+  CU(h, cudaMalloc(&h->muz, N * sizeof(float)));
+  CU(h, cudaMalloc(&h->mrho, N * sizeof(float)));
+  h->stride = stride;
+  h->f_prec = h->cfg.precision;
+  h->f_cells = N;
+  *reallocated = true;
+  return AEROSIM_OK;
+}
+
+int ensure_staging(aerosim_engine* h, size_t bytes) {
+  if (h->staging_bytes >= bytes) return AEROSIM_OK;
+  cudaFree(h->staging);
+  h->staging = nullptr;
+  h->staging_bytes = 0;
+  CU(h, cudaMalloc(&h->staging, bytes));
+  h->staging_bytes = bytes;
+  return AEROSIM_OK;
+}
+
+// Tables of the inlet condition that the reference evaluates with Math.pow and
+// Math.sin (lbmCpuReference.ts:121-125, 334-342), computed once on the host.
+int upload_tables(aerosim_engine* h) {
+  const int ny = h->g.ny;
+  if (h->tab_ny == ny && h->abl) return AEROSIM_OK;
+  cudaFree(h->abl); cudaFree(h->sin_tab);
+  h->abl = nullptr; h->sin_tab = nullptr;
+  std::vector<double> abl(ny), st((size_t)120 * ny);
+  for (int iy = 0; iy < ny; ++iy) {
+    const double yf = (iy + 0.5) / ny;
+    abl[iy] = js_min(1.15, 0.35 + 0.8 * std::pow(yf, 0.3));
+  }
+  for (int s = 0; s < 120; ++s)
+    for (int iy = 0; iy < ny; ++iy)
+      st[(size_t)s * ny + iy] = std::sin(s * 0.15 + ((double)iy / ny) * M_PI * 2.0);
+  CU(h, cudaMalloc(&h->abl, ny * sizeof(double)));
+  CU(h, cudaMalloc(&h->sin_tab, st.size() * sizeof(double)));
+  CU(h, cudaMemcpyAsync(h->abl, abl.data(), ny * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CU(h, cudaMemcpyAsync(h->sin_tab, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  h->tab_ny = ny;
+  return AEROSIM_OK;
+}
+
+// Installs a freshly built device grid (voxelizer output or host upload).
+int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[3], int reset_flow) {
+  // A pending rescale belongs to the old flags: apply it before they change.
+  if (h->have_grid && h->f[0] && !reset_flow) {
+    CU(h, launch_materialize(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->stride, h->g.N,
+                             h->stream));
+    int rc = reset_state(h);
+    if (rc) return rc;
+  }
+  CU(h, cudaMalloc(&ng.cls, std::max<long long>(ng.N, 1)));
+  CU(h, launch_classify(ng.flags, ng.cls, ng.nx, ng.ny, ng.nz, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  free_grid(h->g);
+  h->g = ng;
+  ng = DevGrid();
+  h->have_grid = true;
+  h->dx = dx;
+  h->origin[0] = origin[0]; h->origin[1] = origin[1]; h->origin[2] = origin[2];
+  h->fluid_count = h->g.N - h->g.solid;
+  const long long blocks = std::max<long long>(1, (h->g.B + 255) / 256);
+  if (blocks > h->force_blocks_cap) {
+    cudaFree(h->force_partials);
+    h->force_partials = nullptr;
+    CU(h, cudaMalloc(&h->force_partials, blocks * 8 * sizeof(double)));
+    h->force_blocks_cap = blocks;
+  }
+  int rc = upload_tables(h);
+  if (rc) return rc;
+  bool realloc = false;
+  rc = ensure_pops(h, &realloc);
+  if (rc) return rc;
+  if (reset_flow || realloc) return do_reset(h);
+  return AEROSIM_OK;
+}
+
+void default_config(aerosim_config* c) {
+  // LBMEngine defaults, lbmEngine.ts:42-57
+  c->u_inlet_lattice = 0.085;
+  c->nu_lattice = 0.0005;
+  c->smagorinsky_cs = 0.12;
+  c->ground_no_slip = 0;
+  c->precision = AEROSIM_PREC_F32;
+  c->frontal_area_m2 = M_PI * 0.25;
+  c->characteristic_length_m = 1.0;
+  c->tunnel = aerosim_tunnel{6.0, 2.8, 2.4};
+}
+
+// computeNormalizedForceCoefficients, forceIntegrator.ts:240-315.
+void coefficients(const aerosim_config& c, double dx, aerosim_forces* o) {
+  const double cell_area = dx * dx;
+  const double q_lat = js_max(1e-9, 0.5 * 1.0 * c.u_inlet_lattice * c.u_inlet_lattice);
+  const double a_ref = js_max(1e-4, c.frontal_area_m2 / cell_area);
+  const double l_ref = js_max(1.0, c.characteristic_length_m / dx);
+  o->cd_raw = o->fx / (q_lat * a_ref);
+  o->cl = o->fy / (q_lat * a_ref);
+  o->cm = o->mz / (q_lat * a_ref * l_ref);
+  const double tunnel_area = js_max(1e-4, c.tunnel.width * c.tunnel.height);
+  const double blockage = js_min(0.40, c.frontal_area_m2 / tunnel_area);
+  o->cd = o->cd_raw / (1.0 + 2.5 * js_max(0.0, o->cd_raw) * blockage);
+  const double L = c.characteristic_length_m;
+  o->xcp = std::fabs(o->fy) > 1e-5 ? js_max(-L * 0.5, js_min(L * 0.5, -(o->mz / o->fy) * dx)) : 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aerosim_abi_version(void) { return AEROSIM_ABI_VERSION; }
+
+const char* aerosim_last_error(const aerosim_engine* h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int aerosim_create(int device, aerosim_engine** out) {
+  if (!out) return fail(nullptr, AEROSIM_ERR_ARG, "aerosim_create: out is NULL");
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(nullptr, AEROSIM_ERR_CUDA, std::string("aerosim_create: no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= n) return fail(nullptr, AEROSIM_ERR_ARG, "aerosim_create: bad device ordinal");
+  aerosim_engine* h = new (std::nothrow) aerosim_engine();
+  if (!h) return fail(nullptr, AEROSIM_ERR_NOMEM, "aerosim_create: out of host memory");
+  h->device = device;
+  default_config(&h->cfg);
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
+  if (e == cudaSuccess) e = cudaMalloc(&h->st, sizeof(StepState));
+  if (e == cudaSuccess) e = cudaMalloc(&h->force_ticket, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(&h->force_out, 8 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&h->stats_buf, 4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(h->force_ticket, 0, sizeof(unsigned int));
+  if (e != cudaSuccess) {
+    std::string msg = std::string("aerosim_create: ") + cudaGetErrorString(e);
+    aerosim_destroy(h);
+    return fail(nullptr, AEROSIM_ERR_CUDA, msg);
+  }
+  if (reset_state(h) != AEROSIM_OK) {
+    std::string msg = h->err;
+    aerosim_destroy(h);
+    return fail(nullptr, AEROSIM_ERR_CUDA, msg);
+  }
+  *out = h;
+  return AEROSIM_OK;
+}
+
+int aerosim_destroy(aerosim_engine* h) {
+  if (!h) return AEROSIM_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_grid(h->g);
+  free_pops(h);
+  cudaFree(h->abl); cudaFree(h->sin_tab); cudaFree(h->st);
+  cudaFree(h->force_partials); cudaFree(h->force_ticket); cudaFree(h->force_out);
+  cudaFree(h->stats_buf); cudaFree(h->staging);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return AEROSIM_OK;
+}
+
+int aerosim_voxelize(aerosim_engine* h, const float* positions, int64_t vertex_count,
+                     const int32_t* indices, int64_t index_count, const double* world16,
+                     aerosim_tunnel tunnel, int32_t nx, int32_t ny, int32_t nz, int32_t reset_flow,
+                     aerosim_voxel_info* out) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (nx < 3 || ny < 1 || nz < 1) return fail(h, AEROSIM_ERR_ARG, "aerosim_voxelize: need nx >= 3, ny >= 1, nz >= 1");
+  if ((long long)nx * ny * nz >= (1LL << 31)) return fail(h, AEROSIM_ERR_ARG, "aerosim_voxelize: lattice too large");
+  if (vertex_count < 0 || (vertex_count > 0 && !positions)) return fail(h, AEROSIM_ERR_ARG, "aerosim_voxelize: bad positions");
+  if (indices) {
+    if (index_count < 0) return fail(h, AEROSIM_ERR_ARG, "aerosim_voxelize: bad index_count");
+    for (int64_t i = 0; i < index_count; ++i)
+      if (indices[i] < 0 || indices[i] >= vertex_count)
+        return fail(h, AEROSIM_ERR_ARG, "aerosim_voxelize: index out of range");
+  }
+  if (!(tunnel.height > 0)) return fail(h, AEROSIM_ERR_ARG, "aerosim_voxelize: tunnel height must be > 0");
+  CU(h, cudaSetDevice(h->device));
+  DevGrid ng;
+  std::string e;
+  const int rc = run_voxelizer(positions, vertex_count, indices, index_count, world16, tunnel.height, nx, ny,
+                               nz, h->stream, &ng, &e);
+  if (rc) {
+    free_grid(ng);
+    return fail(h, rc == -4 ? AEROSIM_ERR_DEVICE : AEROSIM_ERR_CUDA, e);
+  }
+  const double origin[3] = {ng.ox, ng.oy, ng.oz};
+  const double dx = ng.h;
+  const int r2 = install_grid(h, ng, dx, origin, reset_flow);
+  free_grid(ng);
+  if (r2) return r2;
+  h->cfg.tunnel = tunnel;
+  return aerosim_get_voxel_info(h, out);
+}
+
+int aerosim_get_voxel_info(aerosim_engine* h, aerosim_voxel_info* out) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (!h->have_grid) return fail(h, AEROSIM_ERR_STATE, "no voxel grid");
+  if (!out) return AEROSIM_OK;
+  out->nx = h->g.nx; out->ny = h->g.ny; out->nz = h->g.nz;
+  out->dx = out->dy = out->dz = h->dx;
+  out->origin_x = h->origin[0]; out->origin_y = h->origin[1]; out->origin_z = h->origin[2];
+  out->solid_cell_count = h->g.solid;
+  out->boundary_cell_count = h->g.B;
+  out->fluid_cell_count = h->g.N - h->g.solid - h->g.B;
+  out->voxelization_time_ms = h->g.vox_ms;
+  return AEROSIM_OK;
+}
+
+int aerosim_read_voxel_grid(aerosim_engine* h, uint8_t* flags, int32_t* bmap, int32_t* bcells, float* q,
+                            float* minq) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (!h->have_grid) return fail(h, AEROSIM_ERR_STATE, "no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  const DevGrid& g = h->g;
+  if (flags) CU(h, cudaMemcpyAsync(flags, g.flags, g.N, cudaMemcpyDeviceToHost, h->stream));
+  if (bmap) CU(h, cudaMemcpyAsync(bmap, g.bmap, g.N * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (g.B > 0) {
+    if (bcells) CU(h, cudaMemcpyAsync(bcells, g.bcells, g.B * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (q) CU(h, cudaMemcpyAsync(q, g.q, g.B * 18 * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (minq) CU(h, cudaMemcpyAsync(minq, g.minq, g.B * 4, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
+int aerosim_set_voxel_grid(aerosim_engine* h, int32_t nx, int32_t ny, int32_t nz, double dx,
+                           const double origin[3], const uint8_t* flags, const int32_t* bmap,
+                           const int32_t* bcells, const float* q, int64_t B, int32_t reset_flow) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (nx < 3 || ny < 1 || nz < 1) return fail(h, AEROSIM_ERR_ARG, "set_voxel_grid: need nx >= 3, ny >= 1, nz >= 1");
+  const long long N = (long long)nx * ny * nz;
+  if (N >= (1LL << 31)) return fail(h, AEROSIM_ERR_ARG, "set_voxel_grid: lattice too large");
+  if (!flags || B < 0 || (B > 0 && (!bcells || !q)))
+    return fail(h, AEROSIM_ERR_ARG, "set_voxel_grid: missing flags / boundary arrays");
+  long long solid = 0;
+  for (long long i = 0; i < N; ++i) {
+    if (flags[i] > 2) return fail(h, AEROSIM_ERR_ARG, "set_voxel_grid: flag value outside {0,1,2}");
+    solid += flags[i] == 1;
+  }
+  std::vector<int32_t> map_built;
+  if (!bmap) {
+    map_built.assign(N, -1);
+    for (int64_t b = 0; b < B; ++b) {
+      if (bcells[b] < 0 || bcells[b] >= N) return fail(h, AEROSIM_ERR_ARG, "set_voxel_grid: boundary cell out of range");
+      map_built[bcells[b]] = (int32_t)b;
+    }
+    bmap = map_built.data();
+  } else {
+    for (long long i = 0; i < N; ++i)
+      if (bmap[i] < -1 || bmap[i] >= B) return fail(h, AEROSIM_ERR_ARG, "set_voxel_grid: boundary index map out of range");
+  }
+  for (int64_t b = 0; b < B; ++b)
+    if (bcells[b] < 0 || bcells[b] >= N) return fail(h, AEROSIM_ERR_ARG, "set_voxel_grid: boundary cell out of range");
+  CU(h, cudaSetDevice(h->device));
+  DevGrid ng;
+  ng.nx = nx; ng.ny = ny; ng.nz = nz; ng.N = N; ng.h = dx;
+  ng.ox = origin ? origin[0] : -nx * dx * 0.5;
+  ng.oy = origin ? origin[1] : -ny * dx * 0.5;
+  ng.oz = origin ? origin[2] : -nz * dx * 0.5;
+  ng.B = B; ng.solid = solid;
+  auto bad = [&](cudaError_t e) {
+    free_grid(ng);
+    return fail(h, AEROSIM_ERR_CUDA, std::string("set_voxel_grid: ") + cudaGetErrorString(e));
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&ng.flags, N)) != cudaSuccess) return bad(e);
+  if ((e = cudaMalloc(&ng.bmap, N * 4)) != cudaSuccess) return bad(e);
+  if ((e = cudaMalloc(&ng.bcells, std::max<int64_t>(B, 1) * 4)) != cudaSuccess) return bad(e);
+  if ((e = cudaMalloc(&ng.q, std::max<int64_t>(B, 1) * 18 * 4)) != cudaSuccess) return bad(e);
+  if ((e = cudaMalloc(&ng.minq, std::max<int64_t>(B, 1) * 4)) != cudaSuccess) return bad(e);
+  std::vector<float> mq(std::max<int64_t>(B, 1), 1.0f);
+  for (int64_t b = 0; b < B; ++b)
+    for (int k = 0; k < 18; ++k) {
+      const float v = q[b * 18 + k];
+      if (v > 0.0f && v < mq[b]) mq[b] = v;
+    }
+  if ((e = cudaMemcpy(ng.flags, flags, N, cudaMemcpyHostToDevice)) != cudaSuccess) return bad(e);
+  if ((e = cudaMemcpy(ng.bmap, bmap, N * 4, cudaMemcpyHostToDevice)) != cudaSuccess) return bad(e);
+  if (B > 0) {
+    if ((e = cudaMemcpy(ng.bcells, bcells, B * 4, cudaMemcpyHostToDevice)) != cudaSuccess) return bad(e);
+    if ((e = cudaMemcpy(ng.q, q, B * 18 * 4, cudaMemcpyHostToDevice)) != cudaSuccess) return bad(e);
+    if ((e = cudaMemcpy(ng.minq, mq.data(), B * 4, cudaMemcpyHostToDevice)) != cudaSuccess) return bad(e);
+  }
+  const double org[3] = {ng.ox, ng.oy, ng.oz};
+  const int rc = install_grid(h, ng, dx, org, reset_flow);
+  free_grid(ng);
+  return rc;
+}
+
+int aerosim_set_config(aerosim_engine* h, const aerosim_config* cfg) {
+  if (!h || !cfg) return AEROSIM_ERR_ARG;
+  if (precision_bytes(cfg->precision) == 0) return fail(h, AEROSIM_ERR_ARG, "set_config: unknown precision");
+  CU(h, cudaSetDevice(h->device));
+  const int old_prec = h->cfg.precision;
+  h->cfg = *cfg;
+  if (h->have_grid && cfg->precision != old_prec) {
+    bool realloc = false;
+    int rc = ensure_pops(h, &realloc);
+    if (rc) return rc;
+    return do_reset(h);
+  }
+  return AEROSIM_OK;
+}
+
+int aerosim_get_config(aerosim_engine* h, aerosim_config* cfg) {
+  if (!h || !cfg) return AEROSIM_ERR_ARG;
+  *cfg = h->cfg;
+  return AEROSIM_OK;
+}
+
+int aerosim_reset_flow(aerosim_engine* h) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (!h->have_grid) return fail(h, AEROSIM_ERR_STATE, "reset_flow: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  return do_reset(h);
+}
+
+int aerosim_step(aerosim_engine* h, int32_t n) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "step: no voxel grid");
+  if (n < 0) return fail(h, AEROSIM_ERR_ARG, "step: negative step count");
+  if (h->step_index + n > 0x7fffffffLL) return fail(h, AEROSIM_ERR_ARG, "step: step index overflow");
+  CU(h, cudaSetDevice(h->device));
+  const DevGrid& g = h->g;
+  StepArgs a{};
+  a.cls = g.cls; a.bmap = g.bmap; a.q = g.q;
+  a.mux = h->mux; a.muy = h->muy; a.muz = h->muz; a.mrho = h->mrho;
+  a.abl = h->abl; a.sin_tab = h->sin_tab; a.st = h->st;
+  a.stride = h->stride; a.fluid_count = h->fluid_count;
+  a.nx = g.nx; a.ny = g.ny; a.nz = g.nz;
+  a.ground_no_slip = h->cfg.ground_no_slip;
+  a.u_inlet = h->cfg.u_inlet_lattice;
+  a.tau0 = 3.0 * h->cfg.nu_lattice + 0.5;
+  const double cs2 = h->cfg.smagorinsky_cs * h->cfg.smagorinsky_cs;
+  a.k_smag = 18.0 * M_SQRT2 * cs2;
+  int tx = ((g.nx + 31) / 32) * 32;
+  if (tx > 256) tx = 256;
+  const int ry = 256 / tx;
+  CU(h, cudaEventRecord(h->ev0, h->stream));
+  for (int s = 0; s < n; ++s) {
+    a.fsrc = h->f[h->cur];
+    a.fdst = h->f[h->cur ^ 1];
+    a.step_index = (int)h->step_index;
+    a.write_macro = (s == n - 1) ? 1 : 0;
+    CU(h, launch_step(h->cfg.precision, a, tx, ry, h->stream));
+    h->cur ^= 1;
+    h->step_index += 1;
+  }
+  CU(h, cudaEventRecord(h->ev1, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  float ms = 0.f;
+  CU(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_ms = ms;
+  h->last_launches = n;
+  return AEROSIM_OK;
+}
+
+int aerosim_get_step_count(aerosim_engine* h, int64_t* out) {
+  if (!h || !out) return AEROSIM_ERR_ARG;
+  *out = h->step_index;
+  return AEROSIM_OK;
+}
+
+int aerosim_read_forces(aerosim_engine* h, aerosim_forces* out) {
+  if (!h || !out) return AEROSIM_ERR_ARG;
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "read_forces: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  double r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (h->g.B > 0) {
+    ForceArgs a{};
+    a.f = h->f[h->cur];
+    a.cls = h->g.cls; a.bcells = h->g.bcells; a.q = h->g.q; a.st = h->st;
+    a.partials = h->force_partials; a.ticket = h->force_ticket; a.out = h->force_out;
+    a.stride = h->stride; a.B = h->g.B;
+    a.nx = h->g.nx; a.ny = h->g.ny; a.nz = h->g.nz;
+    a.prev_slot = prev_slot(h);
+    const unsigned grid = (unsigned)((h->g.B + 255) / 256);
+    CU(h, launch_forces(h->cfg.precision, a, grid, h->stream));
+    CU(h, cudaMemcpyAsync(r, h->force_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->fx = r[0]; out->fy = r[1]; out->fz = r[2];
+  out->mx = r[3]; out->my = r[4]; out->mz = r[5];
+  out->cut_face_links = (int64_t)r[6];
+  out->step = h->step_index;
+  coefficients(h->cfg, h->dx, out);
+  return AEROSIM_OK;
+}
+
+int aerosim_read_macro(aerosim_engine* h, float* ux, float* uy, float* uz, float* rho) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "read_macro: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  const long long N = h->g.N;
+  if (ux) CU(h, cudaMemcpyAsync(ux, h->mux, N * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (uy) CU(h, cudaMemcpyAsync(uy, h->muy, N * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (uz) CU(h, cudaMemcpyAsync(uz, h->muz, N * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (rho) {
+    int rc = ensure_staging(h, N * 4);
+    if (rc) return rc;
+    CU(h, launch_read_macro(h->mrho, h->g.cls, h->st, prev_slot(h), N, (float*)h->staging, h->stream));
+    CU(h, cudaMemcpyAsync(rho, h->staging, N * 4, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
+int aerosim_read_populations(aerosim_engine* h, void* f, int32_t dtype) {
+  if (!h || !f) return AEROSIM_ERR_ARG;
+  if (dtype != AEROSIM_DTYPE_F32 && dtype != AEROSIM_DTYPE_F64) return fail(h, AEROSIM_ERR_ARG, "read_populations: bad dtype");
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "read_populations: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  const long long N = h->g.N;
+  const size_t bytes = (size_t)19 * N * (dtype == AEROSIM_DTYPE_F32 ? 4 : 8);
+  int rc = ensure_staging(h, bytes);
+  if (rc) return rc;
+  CU(h, launch_read_pops(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->stride, N, h->staging,
+                         dtype, h->stream));
+  CU(h, cudaMemcpyAsync(f, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
+int aerosim_write_populations(aerosim_engine* h, const void* f, int32_t dtype) {
+  if (!h || !f) return AEROSIM_ERR_ARG;
+  if (dtype != AEROSIM_DTYPE_F32 && dtype != AEROSIM_DTYPE_F64) return fail(h, AEROSIM_ERR_ARG, "write_populations: bad dtype");
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "write_populations: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  const long long N = h->g.N;
+  const size_t bytes = (size_t)19 * N * (dtype == AEROSIM_DTYPE_F32 ? 4 : 8);
+  int rc = ensure_staging(h, bytes);
+  if (rc) return rc;
+  CU(h, cudaMemcpyAsync(h->staging, f, bytes, cudaMemcpyHostToDevice, h->stream));
+  CU(h, launch_write_pops(h->f_prec, h->f[h->cur], h->stride, N, h->staging, dtype, h->stream));
+  // the written values are final: no rescale is pending on them
+  StepState s{};
+  CU(h, cudaMemcpyAsync(&s, h->st, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  s.apply[0] = s.apply[1] = 0;
+  CU(h, cudaMemcpyAsync(h->st, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
+int aerosim_mass_stats(aerosim_engine* h, aerosim_mass* out) {
+  if (!h || !out) return AEROSIM_ERR_ARG;
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "mass_stats: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  unsigned long long r[4];
+  StepState s{};
+  CU(h, cudaMemsetAsync(h->stats_buf, 0, sizeof(r), h->stream));
+  CU(h, launch_mass_stats(h->mux, h->muy, h->muz, h->mrho, h->g.cls, h->st, prev_slot(h), h->g.N,
+                          h->stats_buf, h->stream));
+  CU(h, cudaMemcpyAsync(r, h->stats_buf, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaMemcpyAsync(&s, h->st, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  std::memset(out, 0, sizeof(*out));
+  const double total = (double)(long long)r[0] * (1.0 / 33554432.0);
+  const long long cnt = (long long)r[1];
+  out->total_mass = total;
+  out->mean_rho = cnt > 0 ? total / (double)cnt : 1.0;
+  double ms;
+  std::memcpy(&ms, &r[2], sizeof(ms));
+  out->max_speed = ms;
+  out->has_nan = (r[3] != 0 || s.nan_seen) ? 1 : 0;
+  out->cumulative_rescale = s.cumulative_rescale;
+  out->rescale_count = s.rescale_count;
+  return AEROSIM_OK;
+}
+
+int aerosim_last_step_timing(aerosim_engine* h, double* ms, int64_t* launches) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (ms) *ms = h->last_ms;
+  if (launches) *launches = h->last_launches;
+  return AEROSIM_OK;
+}
+
+// computeProjectedFrontalArea, frontalArea.ts:22-179: 4x4 supersampled coverage of
+// the projected triangles on a res x res grid over the Y-Z bounding box.
+int aerosim_frontal_area(const float* pos, int64_t nv, const int32_t* idx, int64_t ni, const double* m,
+                         int32_t res, double* out) {
+  if (!out || res <= 0 || nv < 0 || (nv > 0 && !pos)) return AEROSIM_ERR_ARG;
+  *out = 0.0;
+  if (nv < 3) return AEROSIM_OK;
+  const int64_t T = idx ? ni / 3 : nv / 3;
+  if (T == 0) return AEROSIM_OK;
+  std::vector<double> py(nv), pz(nv);
+  double y0 = INFINITY, y1 = -INFINITY, z0 = INFINITY, z1 = -INFINITY;
+  for (int64_t i = 0; i < nv; ++i) {
+    double x = pos[i * 3], y = pos[i * 3 + 1], z = pos[i * 3 + 2];
+    if (m) {
+      const double w = 1.0 / (m[3] * x + m[7] * y + m[11] * z + m[15]);
+      const double ty = (m[1] * x + m[5] * y + m[9] * z + m[13]) * w;
+      const double tz = (m[2] * x + m[6] * y + m[10] * z + m[14]) * w;
+      y = ty; z = tz;
+    }
+    py[i] = y; pz[i] = z;
+    y0 = y < y0 ? y : y0; y1 = y > y1 ? y : y1;
+    z0 = z < z0 ? z : z0; z1 = z > z1 ? z : z1;
+  }
+  const double span_y = y1 - y0, span_z = z1 - z0;
+  if (span_y <= 1e-9 || span_z <= 1e-9) return AEROSIM_OK;
+  std::vector<uint16_t> cover((size_t)res * res, 0);
+  const double sy = res / span_y, sz = res / span_z;
+  static const double sub[4] = {0.125, 0.375, 0.625, 0.875};
+  for (int64_t t = 0; t < T; ++t) {
+    int64_t v[3];
+    for (int k = 0; k < 3; ++k) v[k] = idx ? idx[t * 3 + k] : t * 3 + k;
+    double Z[3], Y[3];
+    for (int k = 0; k < 3; ++k) {
+      if (v[k] < 0 || v[k] >= nv) return AEROSIM_ERR_ARG;
+      Z[k] = (pz[v[k]] - z0) * sz;
+      Y[k] = (py[v[k]] - y0) * sy;
+    }
+    const double area2 = (Z[1] - Z[0]) * (Y[2] - Y[0]) - (Y[1] - Y[0]) * (Z[2] - Z[0]);
+    if (std::fabs(area2) < 1e-11) continue;
+    if (area2 < 0) { std::swap(Z[1], Z[2]); std::swap(Y[1], Y[2]); }
+    const int iz0 = (int)js_max(0, std::floor(js_min(js_min(Z[0], Z[1]), Z[2])));
+    const int iz1 = (int)js_min(res - 1, std::floor(js_max(js_max(Z[0], Z[1]), Z[2])));
+    const int iy0 = (int)js_max(0, std::floor(js_min(js_min(Y[0], Y[1]), Y[2])));
+    const int iy1 = (int)js_min(res - 1, std::floor(js_max(js_max(Y[0], Y[1]), Y[2])));
+    double ez[3], ey[3];
+    for (int k = 0; k < 3; ++k) {
+      ez[k] = Z[(k + 1) % 3] - Z[k];
+      ey[k] = Y[(k + 1) % 3] - Y[k];
+    }
+    for (int iy = iy0; iy <= iy1; ++iy)
+      for (int iz = iz0; iz <= iz1; ++iz) {
+        uint16_t c = cover[(size_t)iy * res + iz];
+        if (c == 0xffff) continue;
+        for (int a = 0; a < 4; ++a)
+          for (int b = 0; b < 4; ++b) {
+            const uint16_t bit = (uint16_t)(1u << (a * 4 + b));
+            if (c & bit) continue;
+            const double Py = iy + sub[a], Pz = iz + sub[b];
+            bool in = true;
+            for (int k = 0; k < 3 && in; ++k) in = ez[k] * (Py - Y[k]) - ey[k] * (Pz - Z[k]) >= -1e-9;
+            if (in) c |= bit;
+          }
+        cover[(size_t)iy * res + iz] = c;
+      }
+  }
+  long long covered = 0;
+  for (uint16_t c : cover) covered += __builtin_popcount(c);
+  *out = ((double)covered / ((double)res * res * 16)) * (span_y * span_z);
+  return AEROSIM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// Internal interfaces between the C-ABI layer and the kernel translation units.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+namespace aerosim {
+
+struct StepArgs;
+struct ForceArgs;
+struct StepState;
+
+// A voxel grid resident on the device (VoxelGridResult, voxelizer.ts:19-59).
+struct DevGrid {
+  int nx = 0, ny = 0, nz = 0;
+  long long N = 0;
+  double h = 0, ox = 0, oy = 0, oz = 0;
+  uint8_t* flags = nullptr;   // reference flags
+  uint8_t* cls = nullptr;     // solver cell classes
+  int32_t* bmap = nullptr;    // boundaryIndexMap
+  int32_t* bcells = nullptr;  // boundaryCellIndices
+  float* q = nullptr;         // boundaryQValues [B * 18]
+  float* minq = nullptr;      // boundaryMinQ
+  long long B = 0, solid = 0;
+  int window[6] = {0, 0, 0, 0, 0, 0};
+  double vox_ms = 0;
+};
+
+// voxelize.cu
+int run_voxelizer(const float* pos, int64_t nverts, const int32_t* idx, int64_t nidx,
+                  const double* world16, double tunnel_height, int nx, int ny, int nz,
+                  cudaStream_t s, DevGrid* g, std::string* err);
+
+// Element size of the population storage of a precision mode.
+size_t precision_bytes(int precision);
+
+// lbm_fast.cu / lbm_exact.cu
+cudaError_t launch_step(int precision, const StepArgs& a, int tx, int ry, cudaStream_t s);
+cudaError_t launch_forces(int precision, const ForceArgs& a, unsigned grid, cudaStream_t s);
+cudaError_t launch_classify(const uint8_t* flags, uint8_t* cls, int nx, int ny, int nz, cudaStream_t s);
+cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, float* mux, float* muy,
+                        float* muz, float* mrho, const double* abl, long long stride, int nx, int ny,
+                        int nz, double u_inlet, int ground_no_slip, cudaStream_t s);
+cudaError_t launch_read_pops(int precision, const void* f, const uint8_t* cls, const StepState* st,
+                             int prev_slot, long long stride, long long N, void* out, int dtype,
+                             cudaStream_t s);
+cudaError_t launch_write_pops(int precision, void* f, long long stride, long long N, const void* in,
+                              int dtype, cudaStream_t s);
+cudaError_t launch_materialize(int precision, void* f, const uint8_t* cls, const StepState* st,
+                               int prev_slot, long long stride, long long N, cudaStream_t s);
+cudaError_t launch_read_macro(const float* mrho, const uint8_t* cls, const StepState* st, int prev_slot,
+                              long long N, float* rho_out, cudaStream_t s);
+cudaError_t launch_mass_stats(const float* mux, const float* muy, const float* muz, const float* rho,
+                              const uint8_t* cls, const StepState* st, int prev_slot, long long N,
+                              unsigned long long* out, cudaStream_t s);
+
+}  // namespace aerosim

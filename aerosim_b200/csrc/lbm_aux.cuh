@@ -1,0 +1,179 @@
+// Solver support kernels: equilibrium initialisation, cell classes, population and
+// macro readback with the pending mean-density rescale, mass statistics.
+#pragma once
+#include "common.cuh"
+#include "lbm_kernels.cuh"
+
+namespace aerosim {
+
+// Cell classes from the reference flags: CLS_NEAR marks non-solid cells for which
+// some clamped pull source clamp(x - c_d), d >= 1, is SOLID (lbmCpuReference.ts:190-196).
+__global__ void classify_kernel(const uint8_t* __restrict__ flags, uint8_t* __restrict__ cls,
+                                int nx, int ny, int nz) {
+  const long long N = (long long)nx * ny * nz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    const uint8_t f = flags[i];
+    uint8_t c = f & CLS_FLAG_MASK;
+    if (f != CELL_SOLID) {
+      const int ix = (int)(i % nx);
+      const long long r = i / nx;
+      const int iy = (int)(r % ny), iz = (int)(r / ny);
+      bool near = false;
+#pragma unroll
+      for (int d = 1; d < 19; ++d) {
+        const int sx = clampi(ix - cx_of(d), 0, nx - 1);
+        const int sy = clampi(iy - cy_of(d), 0, ny - 1);
+        const int sz = clampi(iz - cz_of(d), 0, nz - 1);
+        if (flags[sx + (long long)nx * (sy + (long long)ny * sz)] == CELL_SOLID) near = true;
+      }
+      if (near) c |= CLS_NEAR;
+    }
+    cls[i] = c;
+  }
+}
+
+// resetEquilibrium, lbmCpuReference.ts:114-143: feq(1, (u0, 0, 0)) with u0 the
+// inlet speed (ABL profile when groundNoSlip, 0 at iy = 0) and 0 inside solids.
+template <class S>
+__global__ void init_kernel(void* f0, void* f1, const uint8_t* __restrict__ cls, float* mux,
+                            float* muy, float* muz, float* mrho, const double* abl, long long stride,
+                            int nx, int ny, int nz, double u_inlet, int ground_no_slip) {
+  using T = typename S::T;
+  T* a = static_cast<T*>(f0);
+  T* b = static_cast<T*>(f1);
+  const long long N = (long long)nx * ny * nz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)((i / nx) % ny);
+    double u0 = u_inlet;
+    if (ground_no_slip) {
+      u0 = u_inlet * abl[iy];
+      if (iy == 0) u0 = 0;
+    }
+    if ((cls[i] & CLS_FLAG_MASK) == CELL_SOLID) u0 = 0.0;
+    mux[i] = (float)u0; muy[i] = 0.0f; muz[i] = 0.0f; mrho[i] = 1.0f;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+      const T e = S::raw_of_f(feq64(d, 1.0, u0, 0.0, 0.0), d);
+      a[d * stride + i] = e;
+      b[d * stride + i] = e;
+    }
+  }
+}
+
+// Populations of the latest step with the pending rescale applied to non-solid
+// cells, exactly as the reference's Float32Array holds them after the rescale.
+template <class S, int MODE, class Out>
+__global__ void read_pops_kernel(const void* f, const uint8_t* __restrict__ cls,
+                                 const StepState* st, int prev_slot, long long stride, long long N,
+                                 Out* __restrict__ out) {
+  using T = typename S::T;
+  const T* src = static_cast<const T*>(f);
+  const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
+  const double corr = apply ? st->corr[prev_slot] : 1.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    const bool solid = (cls[i] & CLS_FLAG_MASK) == CELL_SOLID;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+      double v = S::f_of(src[d * stride + i], d);
+      if (!solid && apply) {
+        v = v * corr;
+        if constexpr (MODE == MODE_MIRROR) v = (double)(float)v;
+      }
+      out[d * N + i] = (Out)v;
+    }
+  }
+}
+
+template <class S, class In>
+__global__ void write_pops_kernel(void* f, long long stride, long long N, const In* __restrict__ in) {
+  using T = typename S::T;
+  T* dst = static_cast<T*>(f);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) dst[d * stride + i] = S::raw_of_f((double)in[d * N + i], d);
+  }
+}
+
+// Applies a pending rescale in place (used before the voxel grid changes without a
+// flow reset, so the correction is not later applied with the new flags).
+template <class S, int MODE>
+__global__ void materialize_rescale_kernel(void* f, const uint8_t* __restrict__ cls,
+                                           const StepState* st, int prev_slot, long long stride,
+                                           long long N) {
+  using T = typename S::T;
+  T* dst = static_cast<T*>(f);
+  const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
+  if (!apply) return;
+  const double corr = st->corr[prev_slot];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    if ((cls[i] & CLS_FLAG_MASK) == CELL_SOLID) continue;
+#pragma unroll
+    for (int d = 0; d < 19; ++d)
+      dst[d * stride + i] = S::raw_of_f(S::f_of(dst[d * stride + i], d) * corr, d);
+  }
+}
+
+// Macro readback with the pending rescale on rho (rho[idx] *= corr, :448).
+__global__ void read_macro_kernel(const float* __restrict__ mrho, const uint8_t* __restrict__ cls,
+                                  const StepState* st, int prev_slot, long long N,
+                                  float* __restrict__ rho_out) {
+  const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
+  const double corr = apply ? st->corr[prev_slot] : 1.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    float r = mrho[i];
+    if (apply && (cls[i] & CLS_FLAG_MASK) != CELL_SOLID) r = (float)((double)r * corr);
+    rho_out[i] = r;
+  }
+}
+
+// computeFluidMassStats (lbmCpuReference.ts:461-495) on the rescaled densities: exact
+// fixed-point density sum,
+// fluid count, max speed (ordered as unsigned bit patterns of non-negative doubles)
+// and a NaN flag.  out: [sum_fixed, count, max_speed_bits, nan]
+__global__ void mass_stats_kernel(const float* __restrict__ mux, const float* __restrict__ muy,
+                                  const float* __restrict__ muz, const float* __restrict__ rho,
+                                  const uint8_t* __restrict__ cls, const StepState* st,
+                                  int prev_slot, long long N, unsigned long long* out) {
+  const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
+  const double corr = apply ? st->corr[prev_slot] : 1.0;
+  long long s = 0, cnt = 0;
+  double mx = 0.0;
+  int nan = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    if ((cls[i] & CLS_FLAG_MASK) == CELL_SOLID) continue;
+    float r = rho[i];
+    if (apply) r = (float)((double)r * corr);
+    const float u = mux[i], v = muy[i], w = muz[i];
+    if (r != r || u != u || v != v || w != w) {
+      nan = 1;
+      continue;
+    }
+    s += llrint((double)r * 33554432.0);
+    ++cnt;
+    const double du = u, dv = v, dw = w;
+    const double sp = sqrt(du * du + dv * dv + dw * dw);
+    if (sp > mx) mx = sp;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  }
+  nan = __any_sync(0xffffffffu, nan);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&out[0], (unsigned long long)s);
+    atomicAdd(&out[1], (unsigned long long)cnt);
+    atomicMax(&out[2], (unsigned long long)__double_as_longlong(mx));
+    if (nan) atomicOr(&out[3], 1ull);
+  }
+}
+
+}  // namespace aerosim

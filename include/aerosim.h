@@ -1,0 +1,185 @@
+/*
+ * aerosim.h -- C ABI of the B200-native AeroSim solver hot path (libaerosim.so).
+ *
+ * The library replaces the WebGPU compute path of the reference application
+ * (necrolingus/aerosim): the D3Q19 regularized-BGK + Smagorinsky stream/collide
+ * step with Bouzidi curved walls, the domain boundary conditions and mass
+ * rescale, the momentum-exchange force reduction, and the BVH triangle
+ * voxelizer.  Every entry point returns an int status (AEROSIM_OK == 0,
+ * negative on error); aerosim_last_error() returns a message for the handle.
+ *
+ * Ownership: the caller owns every host buffer passed in or out; the library
+ * owns all device memory behind an aerosim_engine handle.  Calls on one handle
+ * are not thread-safe (the reference serialises steps with an isBusy flag,
+ * src/solver/lbmEngine.ts:420,478).  Each handle owns one CUDA stream; every
+ * call returns after its device work is complete.
+ *
+ * Cell indexing everywhere: idx = ix + nx * (iy + ny * iz); populations are
+ * structure-of-arrays, direction d of cell idx at f[d * nx*ny*nz + idx]
+ * (src/solver/lbmCpuReference.ts:138, shaders/collideStream.wgsl:2).
+ */
+#ifndef AEROSIM_H_
+#define AEROSIM_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AEROSIM_ABI_VERSION 1
+
+enum aerosim_status {
+  AEROSIM_OK = 0,
+  AEROSIM_ERR_ARG = -1,       /* invalid argument or inconsistent voxel grid */
+  AEROSIM_ERR_STATE = -2,     /* call out of order (e.g. step before a voxel grid) */
+  AEROSIM_ERR_CUDA = -3,      /* CUDA runtime error */
+  AEROSIM_ERR_DEVICE = -4,    /* a kernel reported an error status */
+  AEROSIM_ERR_NOMEM = -5      /* device allocation failed */
+};
+
+/* Cell flags, src/geometry/voxelizer.ts:12-14 */
+enum aerosim_cell_flag { AEROSIM_CELL_FLUID = 0, AEROSIM_CELL_SOLID = 1, AEROSIM_CELL_BOUNDARY = 2 };
+
+/* Population storage / arithmetic of the solver. */
+enum aerosim_precision {
+  AEROSIM_PREC_F32 = 0,        /* FP32 storage, FP32 collision (the production path) */
+  AEROSIM_PREC_F32_MIRROR = 1, /* FP32 storage, FP64 arithmetic rounded exactly like the
+                                  reference's JavaScript CPU solver (bit-parity mode) */
+  AEROSIM_PREC_F16S = 2,       /* FP16 storage of (f - w) scaled by 2^15, FP32 collision */
+  AEROSIM_PREC_BF16S = 3,      /* BF16 storage of (f - w), FP32 collision */
+  AEROSIM_PREC_F64 = 4         /* FP64 storage and arithmetic (the GPU FP64 oracle run) */
+};
+
+/* Element type for population read/write. */
+enum aerosim_dtype { AEROSIM_DTYPE_F32 = 0, AEROSIM_DTYPE_F64 = 1 };
+
+typedef struct aerosim_engine aerosim_engine;
+
+/* TunnelDimensions, src/core/types.ts:73 */
+typedef struct {
+  double length, width, height; /* metres */
+} aerosim_tunnel;
+
+/* Scalar part of VoxelGridResult, src/geometry/voxelizer.ts:19-59 */
+typedef struct {
+  int32_t nx, ny, nz;
+  double dx, dy, dz;
+  double origin_x, origin_y, origin_z;
+  int64_t solid_cell_count, boundary_cell_count, fluid_cell_count;
+  double voxelization_time_ms;
+} aerosim_voxel_info;
+
+/* Solver part of LBMSolverConfig, src/solver/lbmEngine.ts:17-32 */
+typedef struct {
+  double u_inlet_lattice;          /* uInletLattice */
+  double nu_lattice;               /* nuLattice */
+  double smagorinsky_cs;           /* smagorinskyCs */
+  int32_t ground_no_slip;          /* groundNoSlip */
+  int32_t precision;               /* enum aerosim_precision */
+  double frontal_area_m2;          /* frontalAreaM2 (A_ref) */
+  double characteristic_length_m;  /* characteristicLengthM (L_ref) */
+  aerosim_tunnel tunnel;           /* tunnel */
+} aerosim_config;
+
+/* Raw momentum-exchange sums (lattice units) and the normalized coefficients of
+ * integrateLatticeMomentumExchange / computeNormalizedForceCoefficients,
+ * src/solver/forceIntegrator.ts:106-315.  Moments are about the domain centre. */
+typedef struct {
+  double fx, fy, fz;
+  double mx, my, mz;
+  double cd_raw, cd, cl, cm, xcp;
+  int64_t cut_face_links;
+  int64_t step;
+} aerosim_forces;
+
+/* computeFluidMassStats, src/solver/lbmCpuReference.ts:461-495, plus the
+ * cumulative product and count of the mean-density rescales (:434-455). */
+typedef struct {
+  double total_mass, mean_rho, max_speed;
+  int32_t has_nan;
+  int32_t reserved;
+  double cumulative_rescale;
+  int64_t rescale_count;
+} aerosim_mass;
+
+/* ---- lifetime ------------------------------------------------------------ */
+
+/* new LBMEngine(device), src/solver/lbmEngine.ts:92.  device = CUDA ordinal. */
+int aerosim_create(int device, aerosim_engine** out);
+int aerosim_destroy(aerosim_engine* h);
+/* Message of the last failing call on h (or of the last failing aerosim_create when
+ * h is NULL).  The pointer stays valid until the next call on h. */
+const char* aerosim_last_error(const aerosim_engine* h);
+int aerosim_abi_version(void);
+
+/* ---- geometry -> lattice ------------------------------------------------ */
+
+/* voxelizeMeshToLattice(geometry, worldMatrix, tunnel, grid), voxelizer.ts:86-281,
+ * run on the GPU.  positions: float xyz per vertex (BufferGeometry 'position');
+ * indices: optional triangle index list (NULL for a triangle soup); world16:
+ * optional column-major 4x4 matrix (THREE.Matrix4.elements) or NULL.  The result
+ * stays on the device and becomes the engine's voxel grid, as setVoxelGrid would
+ * install it (lbmEngine.ts:142-287); reset_flow re-initialises the populations. */
+int aerosim_voxelize(aerosim_engine* h, const float* positions, int64_t vertex_count,
+                     const int32_t* indices, int64_t index_count, const double* world16,
+                     aerosim_tunnel tunnel, int32_t nx, int32_t ny, int32_t nz,
+                     int32_t reset_flow, aerosim_voxel_info* out);
+
+/* Copies the engine's voxel grid to host arrays (any pointer may be NULL):
+ * flags u8[N], boundary_index_map i32[N], boundary_cells i32[B], q f32[B*18]
+ * (index bIdx*18 + d-1), min_q f32[B]. */
+int aerosim_read_voxel_grid(aerosim_engine* h, uint8_t* flags, int32_t* boundary_index_map,
+                            int32_t* boundary_cells, float* q, float* min_q);
+int aerosim_get_voxel_info(aerosim_engine* h, aerosim_voxel_info* out);
+
+/* setVoxelGrid(voxel, config, resetFlow), lbmEngine.ts:142-287, from host arrays
+ * of a VoxelGridResult.  boundary_index_map may be NULL (rebuilt from the list). */
+int aerosim_set_voxel_grid(aerosim_engine* h, int32_t nx, int32_t ny, int32_t nz, double dx,
+                           const double origin[3], const uint8_t* flags,
+                           const int32_t* boundary_index_map, const int32_t* boundary_cells,
+                           const float* q, int64_t boundary_count, int32_t reset_flow);
+
+/* ---- solver --------------------------------------------------------------- */
+
+/* updateConfig(config), lbmEngine.ts:289-300.  A precision change re-allocates the
+ * population buffers and re-initialises the flow. */
+int aerosim_set_config(aerosim_engine* h, const aerosim_config* cfg);
+int aerosim_get_config(aerosim_engine* h, aerosim_config* cfg);
+/* resetFlow(), lbmEngine.ts:677-688 (resetEquilibrium, lbmCpuReference.ts:114-143). */
+int aerosim_reset_flow(aerosim_engine* h);
+/* The substep loop of stepAndExtractSlice, lbmEngine.ts:483-527 (step(n),
+ * lbmCpuReference.ts:145-156): n x (stream/collide, boundaries, mass rescale). */
+int aerosim_step(aerosim_engine* h, int32_t n);
+/* getStepCount(), lbmEngine.ts:690. */
+int aerosim_get_step_count(aerosim_engine* h, int64_t* out);
+/* Force readout of stepAndExtractSlice, lbmEngine.ts:555-658: FP64 momentum exchange
+ * on the device, coefficients with the configured A_ref, L_ref and tunnel. */
+int aerosim_read_forces(aerosim_engine* h, aerosim_forces* out);
+/* macroField readback (readMacroField = true), lbmEngine.ts:577-625. */
+int aerosim_read_macro(aerosim_engine* h, float* ux, float* uy, float* uz, float* rho);
+/* Populations of the latest step (fSrc after the swap) as f32 or f64, 19*N values. */
+int aerosim_read_populations(aerosim_engine* h, void* f, int32_t dtype);
+int aerosim_write_populations(aerosim_engine* h, const void* f, int32_t dtype);
+/* computeFluidMassStats, lbmCpuReference.ts:461-495. */
+int aerosim_mass_stats(aerosim_engine* h, aerosim_mass* out);
+
+/* ---- timing support -------------------------------------------------------- */
+
+/* Device time of the last aerosim_step call in milliseconds (CUDA events on the
+ * engine's stream) and the number of kernels it launched. */
+int aerosim_last_step_timing(aerosim_engine* h, double* ms, int64_t* kernel_launches);
+
+/* ---- host-side geometry inputs ------------------------------------------- */
+
+/* computeProjectedFrontalArea(geometry, worldMatrix, gridResolution),
+ * src/geometry/frontalArea.ts:22-179 (A_ref). */
+int aerosim_frontal_area(const float* positions, int64_t vertex_count, const int32_t* indices,
+                         int64_t index_count, const double* world16, int32_t grid_resolution,
+                         double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AEROSIM_H_ */

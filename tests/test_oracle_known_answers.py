@@ -1,0 +1,217 @@
+"""The reference's own known-answer tests, re-run against the CPU oracle.
+
+These pin the oracle (a restatement of the reference's TypeScript CPU path) to the
+answers the reference's test suite asserts:
+  phase2.test.ts:42-60    1 m cube -> 8000 solid cells, > 2400 boundary cells
+  phase2.test.ts:62-82    non-manifold cube, 3-ray vote
+  phase2.test.ts:84-129   analytic sphere q error < 1e-4 over > 1000 links
+  phase4.test.ts:52-117   link consistency and the q / -1 sentinel
+  phase4.test.ts:11-50    zero inflow -> zero force
+  phase3.test.ts:8-43     Re = 1e5 mass conservation, 10 000 steps
+  phase3.test.ts:45-124   Karman street Strouhal number
+  phase4.test.ts:119-159  Cd bands of the calibration bodies (testRunner.ts:39-155)
+The meshes are this project's generators standing in for the three.js presets.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from aerosim_b200 import meshes
+
+CX = [0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0]
+CY = [0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1]
+CZ = [0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1]
+
+
+def test_cube_solid_count(oracle_mod):
+    v = oracle_mod.voxelize(meshes.box(1.0, 1.0, 1.0, 4), None, 2.0, 80, 40, 40)
+    assert v.solid == 8000
+    assert v.boundary_count > 2400
+    assert v.flags[40 + 80 * (20 + 40 * 20)] == 1
+    assert v.flags[2 + 80 * (2 + 40 * 2)] == 0
+
+
+def test_non_manifold_vote(oracle_mod):
+    soup = meshes.as_soup(meshes.box(1.0, 1.0, 1.0, 4))[:-3]
+    b = oracle_mod.BVH((soup, None))
+    assert b.is_point_inside(0.0, 0.0, 0.0)
+    assert b.is_point_inside(0.2, -0.1, 0.15)
+    assert not b.is_point_inside(0.8, 0.0, 0.0)
+    assert not b.is_point_inside(0.0, 0.9, 0.0)
+
+
+def _sphere_q_exact(f, v, r):
+    a = v @ v
+    b = 2.0 * (f @ v)
+    c = f @ f - r * r
+    disc = b * b - 4 * a * c
+    if disc < 0:
+        return -1.0
+    s = math.sqrt(disc)
+    for t in ((-b - s) / (2 * a), (-b + s) / (2 * a)):
+        if 0 <= t <= 1.0:
+            return t
+    return -1.0
+
+
+def test_analytic_sphere_q(oracle_mod):
+    R = 0.5
+    v = oracle_mod.voxelize(meshes.uv_sphere(R, 840, 560), None, 2.0, 40, 40, 40)
+    assert v.boundary_count > 500
+    errs = []
+    for b, ci in enumerate(v.bcells):
+        ix = ci % 40
+        iy = (ci // 40) % 40
+        iz = ci // 1600
+        f = np.array([v.origin[0] + (ix + 0.5) * v.dx, v.origin[1] + (iy + 0.5) * v.dx,
+                      v.origin[2] + (iz + 0.5) * v.dx])
+        for d in range(1, 19):
+            qm = v.q[b * 18 + d - 1]
+            if qm < 0:
+                continue
+            qe = _sphere_q_exact(f, np.array([CX[d], CY[d], CZ[d]]) * v.dx, R)
+            if qe > 0:
+                errs.append(abs(qm - qe))
+    assert len(errs) > 1000
+    assert np.mean(errs) < 1e-4
+
+
+@pytest.mark.parametrize("name", ["sphere", "cube", "cylinder", "ellipsoid", "naca"])
+def test_link_consistency(oracle_mod, name):
+    mesh = {
+        "sphere": lambda: meshes.uv_sphere(0.5, 96, 64),
+        "cube": lambda: meshes.box(1.0, 1.0, 1.0, 4),
+        "cylinder": lambda: meshes.cylinder(0.3, 1.2, 80, 4),
+        "ellipsoid": lambda: meshes.perturbed_ellipsoid((0.9, 0.4, 0.3), 0.04, 0, 4),
+        "naca": lambda: meshes.naca0012_wing(1.2, 1.6, 15.0),
+    }[name]()
+    nx, ny, nz = 54, 27, 27
+    v = oracle_mod.voxelize(mesh, None, 2.7, nx, ny, nz)
+    flags = v.flags.reshape(nz, ny, nx)
+    solid = np.pad(flags == 1, 1)
+    fluid = flags == 0
+    for d in range(1, 19):
+        nb = solid[1 + CZ[d]:1 + CZ[d] + nz, 1 + CY[d]:1 + CY[d] + ny, 1 + CX[d]:1 + CX[d] + nx]
+        assert not np.any(fluid & nb), f"fluid cell touches solid along link {d}"
+    for b, ci in enumerate(v.bcells):
+        ix, iy, iz = ci % nx, (ci // nx) % ny, ci // (nx * ny)
+        for d in range(1, 19):
+            a, bb, c = ix + CX[d], iy + CY[d], iz + CZ[d]
+            q = v.q[b * 18 + d - 1]
+            if 0 <= a < nx and 0 <= bb < ny and 0 <= c < nz:
+                if flags[c, bb, a] == 1:
+                    assert 0.0 < q <= 1.0
+                else:
+                    assert q == -1.0
+
+
+def test_zero_inflow_zero_force(oracle_mod):
+    mesh = meshes.uv_sphere(0.5, 96, 64)
+    v = oracle_mod.voxelize(mesh, None, 2.4, 48, 24, 24)
+    s = oracle_mod.Solver(v, u_inlet=0.0, nu=0.005)
+    s.step(5)
+    me = oracle_mod.momentum_exchange(v, s.f(0))
+    a = oracle_mod.frontal_area(mesh)
+    co = oracle_mod.force_coefficients(me["fx"], me["fy"], me["mz"], v.dx, 0.08, a, 1.0, 2.4, 2.4)
+    for k in ("fx", "fy", "fz"):
+        assert abs(me[k]) < 1e-6
+    assert abs(co["cdRaw"]) < 1e-6 and abs(co["cl"]) < 1e-6
+
+
+def test_mass_conservation_re1e5(oracle_mod):
+    v = oracle_mod.voxelize(meshes.uv_sphere(0.5, 96, 64), None, 2.0, 16, 8, 8)
+    u = 0.09
+    s = oracle_mod.Solver(v, u_inlet=u, nu=u * 6.0 / 1e5, cs=0.14)
+    st = s.mass_stats()
+    assert not st["hasNaN"] and abs(st["meanRho"] - 1.0) < 5e-4
+    s.step(10000, threads=oracle_mod.max_threads())
+    st = s.mass_stats()
+    assert not st["hasNaN"]
+    assert abs(st["meanRho"] - 1.0) < 0.015
+    assert 0.01 < st["maxSpeed"] < 0.25
+
+
+def test_karman_strouhal(oracle_mod):
+    D = 0.25
+    cyl = meshes.cylinder(D / 2, 1.0, 64, 1, axis=2)
+    world = [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, -1.2, 0, 0, 1]
+    v = oracle_mod.voxelize(cyl, world, 2.0, 96, 40, 3)
+    u = 0.10
+    s = oracle_mod.Solver(v, u_inlet=u, nu=u * 5.0 / 180.0, cs=0.04)
+    probe = 39 + 96 * (20 + 40 * 1)
+    t = oracle_mod.max_threads()
+    s.step(700, threads=t)
+    uy = np.empty(1400)
+    for i in range(1400):
+        s.step(1, threads=t)
+        uy[i] = s.macro()["uy"][probe]
+    uy -= uy.mean()
+    cross = [i - 1 + (-uy[i - 1]) / max(1e-12, uy[i] - uy[i - 1])
+             for i in range(1, 1400) if uy[i - 1] <= 0 < uy[i]]
+    assert np.abs(uy).max() > 1e-4
+    assert len(cross) >= 2
+    period = (cross[-1] - cross[0]) / (len(cross) - 1)
+    st = (1.0 / period) * 5.0 / u
+    assert 0.14 < st < 0.25
+
+
+def _sphere_cd_target(re):
+    re = max(0.1, re)
+    return (24.0 / re) * (1.0 + 0.15 * re ** 0.687) + 0.42 / (1.0 + 42500.0 * re ** -1.16)
+
+
+def _ogive():
+    L, body, R = 1.0, 0.4, 0.25
+    rho = (R * R + L * L) / (2 * R)
+    pts = [(max(0.0, math.sqrt(max(0.0, rho * rho - (L - x) ** 2)) + R - rho), x)
+           for x in np.linspace(0, L, 61)]
+    pts += [(R, L + body), (0.0, L + body)]
+    pos, idx = meshes.lathe(np.array(pts), 72)
+    p = pos.astype(np.float64)
+    p = np.stack([p[:, 1], -p[:, 0], p[:, 2]], 1)  # rotate -90 deg about z: tip at -x
+    p -= (p.max(0) + p.min(0)) / 2
+    return p.astype(np.float32), idx
+
+
+BANDS = {  # testRunner.ts / analyticalCases.ts:21-134
+    "cube": (lambda: meshes.box(1.0, 1.0, 1.0, 4), lambda re: (0.88, 1.22)),
+    "sphere": (lambda: meshes.uv_sphere(0.5, 96, 64),
+               lambda re: (round(_sphere_cd_target(re), 3) * 0.78, round(_sphere_cd_target(re), 3) * 1.25)),
+    "cylinder": (lambda: meshes.cylinder(0.3, 1.2, 80, 4),
+                 lambda re: ((0.68 + 5.5 / math.sqrt(re)) * 0.8, (0.68 + 5.5 / math.sqrt(re)) * 1.2)),
+    "rocket_nose": (_ogive, lambda re: ((0.2 + 26 / math.sqrt(re)) * 0.8, (0.2 + 26 / math.sqrt(re)) * 1.25)),
+}
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("name", sorted(BANDS))
+def test_cd_band(oracle_mod, name):
+    """runSinglePhysicsBenchmark (testRunner.ts:39-155): 60x36x36, sine^2 ramp over 80
+    steps to u = 0.08, nu = 0.002, Cs = 0.12, 350 steps, mean Cd over a 40-sample window."""
+    from aerosim_b200.forces import AIR_20C, ForceConvergenceTracker
+    make, band = BANDS[name]
+    mesh = make()
+    v = oracle_mod.voxelize(mesh, None, 3.6, 60, 36, 36)
+    a_ref = oracle_mod.frontal_area(mesh)
+    pos = mesh[0]
+    l_ref = max(1e-4, float(pos[:, 0].max() - pos[:, 0].min()))
+    u, nu = 0.08, 0.002
+    re = round((u * (l_ref / v.dx)) / nu)
+    s = oracle_mod.Solver(v, u_inlet=0.001, nu=nu, cs=0.12)
+    tr = ForceConvergenceTracker()
+    tr.reset(40)
+    out = None
+    t = oracle_mod.max_threads()
+    for step in range(1, 351):
+        s.set_params(u_inlet=u * math.sin(0.5 * math.pi * step / 80) ** 2 if step <= 80 else u)
+        s.step(1, threads=t)
+        if step > 175:
+            me = oracle_mod.momentum_exchange(v, s.f(0))
+            co = oracle_mod.force_coefficients(me["fx"], me["fy"], me["mz"], v.dx, u, a_ref, l_ref, 3.6, 3.6)
+            out = tr.push_sample(step, co["cd"], co["cl"], co["cm"], co["xcp"], 25.0, AIR_20C, a_ref)
+    cd = round(out["meanCd"], 3)
+    lo, hi = band(re)
+    assert lo <= cd <= hi, (name, cd, lo, hi, re)
+    if name in ("cube", "sphere"):
+        assert abs(round(out["meanCl"], 3)) <= 0.02
