@@ -57,8 +57,13 @@ constexpr float F16S_INV_SCALE = 1.0f / 32768.0f;
 //   h_of(raw, d), raw_of_h(h, d)  -- float deviation
 //   f_of(raw, d), raw_of_f(f, d)  -- double value
 // d is a loop index of fully unrolled loops, so w_d folds to a constant.
+// h_scaled(raw, d, corr, corr_s) returns f * corr - w_d in one fused step (the
+// pending mean-density rescale folded into the load; corr_s = corr / 2^15).
 struct StoreF32 {
   using T = float;
+  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
+    return fmaf(v, corr, -wf_of(d));
+  }
   __device__ __forceinline__ static float h_of(T v, int d) { return v - wf_of(d); }
   __device__ __forceinline__ static T raw_of_h(float h, int d) { return wf_of(d) + h; }
   __device__ __forceinline__ static double f_of(T v, int) { return (double)v; }
@@ -66,6 +71,9 @@ struct StoreF32 {
 };
 struct StoreF64 {
   using T = double;
+  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
+    return (float)(v * (double)corr - w64_of(d));
+  }
   __device__ __forceinline__ static float h_of(T v, int d) { return (float)(v - w64_of(d)); }
   __device__ __forceinline__ static T raw_of_h(float h, int d) { return w64_of(d) + (double)h; }
   __device__ __forceinline__ static double f_of(T v, int) { return v; }
@@ -73,6 +81,9 @@ struct StoreF64 {
 };
 struct StoreF16S {
   using T = __half;
+  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float corr_s) {
+    return fmaf(__half2float(v), corr_s, wf_of(d) * (corr - 1.0f));
+  }
   __device__ __forceinline__ static float h_of(T v, int) { return __half2float(v) * F16S_INV_SCALE; }
   __device__ __forceinline__ static T raw_of_h(float h, int) { return __float2half_rn(h * F16S_SCALE); }
   __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)h_of(v, d); }
@@ -80,11 +91,41 @@ struct StoreF16S {
 };
 struct StoreBF16S {
   using T = __nv_bfloat16;
+  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
+    return fmaf(__bfloat162float(v), corr, wf_of(d) * (corr - 1.0f));
+  }
   __device__ __forceinline__ static float h_of(T v, int) { return __bfloat162float(v); }
   __device__ __forceinline__ static T raw_of_h(float h, int) { return __float2bfloat16_rn(h); }
   __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)h_of(v, d); }
   __device__ __forceinline__ static T raw_of_f(double f, int d) { return raw_of_h((float)(f - (double)wf_of(d)), d); }
 };
+
+// Solver memory layout.  Populations: plane d starts at d * plane; within a plane the
+// x-rows (iy, iz) are `pitch` elements apart (pitch = nx rounded up to 16, so every
+// row starts on a 16-byte boundary for the bulk copies).  The cell-class array uses
+// the same row pitch in bytes.
+struct Layout {
+  long long plane;  // elements per direction plane
+  int pitch;        // elements per x-row
+  int nx, ny, nz;
+  __host__ __device__ long long row_of(long long cell) const { return cell / nx; }
+  __host__ __device__ long long at(int d, long long cell) const {
+    const long long r = cell / nx;
+    return (long long)d * plane + r * pitch + (cell - r * nx);
+  }
+  __host__ __device__ long long cls_at(long long cell) const {
+    const long long r = cell / nx;
+    return r * pitch + (cell - r * nx);
+  }
+};
+
+__host__ inline Layout make_layout(int nx, int ny, int nz) {
+  Layout L;
+  L.nx = nx; L.ny = ny; L.nz = nz;
+  L.pitch = (nx + 15) / 16 * 16;
+  L.plane = (long long)ny * nz * L.pitch;
+  return L;
+}
 
 // Device-resident solver state shared across steps.  Slot [s & 1] belongs to step s.
 struct StepState {

@@ -3,6 +3,7 @@
 // kernels.  Host code only; every device buffer is owned by the engine handle.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -28,7 +29,15 @@ struct aerosim_engine {
   void* f[2] = {nullptr, nullptr};
   int cur = 0;                 // f[cur] holds the latest populations (fSrc)
   int f_prec = -1;
-  long long f_cells = 0, stride = 0;
+  long long f_cells = 0;
+  Layout L{};
+  // persistent step-kernel launch shape
+  dim3 block{256, 1, 1};
+  unsigned grid = 1;
+  size_t smem = 0;
+  int stages = 3;
+  int occupancy = 0;
+  int num_sms = 148;
   float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
   double* abl = nullptr;
   double* sin_tab = nullptr;
@@ -93,7 +102,7 @@ int reset_state(aerosim_engine* h) {
 int do_reset(aerosim_engine* h) {
   const DevGrid& g = h->g;
   CU(h, launch_init(h->cfg.precision, h->f[0], h->f[1], g.cls, h->mux, h->muy, h->muz, h->mrho, h->abl,
-                    h->stride, g.nx, g.ny, g.nz, h->cfg.u_inlet_lattice, h->cfg.ground_no_slip, h->stream));
+                    h->L, h->cfg.u_inlet_lattice, h->cfg.ground_no_slip, h->stream));
   h->cur = 0;
   h->step_index = 0;
   int rc = reset_state(h);
@@ -102,25 +111,64 @@ int do_reset(aerosim_engine* h) {
   return AEROSIM_OK;
 }
 
+// Chooses the persistent step-kernel launch: CTAs of 8 consumer warps + 1 producer
+// warp, as many resident per SM as registers and shared memory allow, and the
+// deepest shared-memory ring (up to 4 slots) that keeps that residency.
+int configure_step(aerosim_engine* h) {
+  const Layout& L = h->L;
+  const size_t eb = precision_bytes(h->cfg.precision);
+  const dim3 block(kStepThreads, 1, 1);
+  StepArgs dummy{};
+  const char* env = getenv("AEROSIM_STAGES");
+  const int forced = env ? atoi(env) : 0;
+  int best_s = 0, best_occ = 0;
+  for (int S = 2; S <= 8; ++S) {
+    if (forced && S != forced) continue;
+    const size_t smem = step_smem_bytes(L, S, eb);
+    if (smem > 227 * 1024) break;
+    int occ = 0;
+    cudaError_t e = launch_step(h->cfg.precision, dummy, block, 0, smem, h->stream, &occ);
+    if (e != cudaSuccess || occ < 1) break;
+    // keep deepening the ring while the residency does not drop
+    if (best_s == 0 || (occ >= best_occ && S <= 4)) {
+      best_s = S;
+      best_occ = occ;
+    }
+  }
+  if (best_s == 0) return fail(h, AEROSIM_ERR_ARG, "step kernel: no launch configuration fits shared memory");
+  h->block = block;
+  h->stages = best_s;
+  h->smem = step_smem_bytes(L, best_s, eb);
+  // the probes above raised the shared-memory attribute to their own sizes: set it
+  // (and the occupancy) for the chosen configuration
+  CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ));
+  h->occupancy = best_occ;
+  const long long items = ((long long)L.ny * L.nz + rows_per_item(L.nx) - 1) / rows_per_item(L.nx);
+  long long grid = (long long)best_occ * h->num_sms;
+  const char* genv = getenv("AEROSIM_CTAS_PER_SM");
+  if (genv && atoi(genv) > 0 && atoi(genv) <= best_occ) grid = (long long)atoi(genv) * h->num_sms;
+  if (grid > items) grid = items;
+  h->grid = (unsigned)(grid < 1 ? 1 : grid);
+  return AEROSIM_OK;
+}
+
 // Allocates population and macro buffers for the current grid and precision.
 int ensure_pops(aerosim_engine* h, bool* reallocated) {
   *reallocated = false;
   const long long N = h->g.N;
-  if (h->f[0] && h->f_prec == h->cfg.precision && h->f_cells == N) return AEROSIM_OK;
+  if (h->f[0] && h->f_prec == h->cfg.precision && h->f_cells == N) return configure_step(h);
   free_pops(h);
   const size_t eb = precision_bytes(h->cfg.precision);
-  const long long stride = (N + 63) / 64 * 64;  // 256-byte aligned direction planes (FP32)
-  CU(h, cudaMalloc(&h->f[0], 19 * (size_t)stride * eb));
-  CU(h, cudaMalloc(&h->f[1], 19 * (size_t)stride * eb));
+  CU(h, cudaMalloc(&h->f[0], 19 * (size_t)h->L.plane * eb));
+  CU(h, cudaMalloc(&h->f[1], 19 * (size_t)h->L.plane * eb));
   CU(h, cudaMalloc(&h->mux, N * sizeof(float)));
   CU(h, cudaMalloc(&h->muy, N * sizeof(float)));
   CU(h, cudaMalloc(&h->muz, N * sizeof(float)));
   CU(h, cudaMalloc(&h->mrho, N * sizeof(float)));
-  h->stride = stride;
   h->f_prec = h->cfg.precision;
   h->f_cells = N;
   *reallocated = true;
-  return AEROSIM_OK;
+  return configure_step(h);
 }
 
 int ensure_staging(aerosim_engine* h, size_t bytes) {
@@ -161,16 +209,20 @@ int upload_tables(aerosim_engine* h) {
 int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[3], int reset_flow) {
   // A pending rescale belongs to the old flags: apply it before they change.
   if (h->have_grid && h->f[0] && !reset_flow) {
-    CU(h, launch_materialize(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->stride, h->g.N,
+    CU(h, launch_materialize(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->L, h->g.N,
                              h->stream));
     int rc = reset_state(h);
     if (rc) return rc;
   }
-  CU(h, cudaMalloc(&ng.cls, std::max<long long>(ng.N, 1)));
-  CU(h, launch_classify(ng.flags, ng.cls, ng.nx, ng.ny, ng.nz, h->stream));
+  const Layout nl = make_layout(ng.nx, ng.ny, ng.nz);
+  CU(h, cudaMalloc(&ng.cls, std::max<long long>((long long)ng.ny * ng.nz * nl.pitch, 1)));
+  CU(h, cudaMemsetAsync(ng.cls, CELL_SOLID, (size_t)ng.ny * ng.nz * nl.pitch, h->stream));
+  CU(h, launch_classify(ng.flags, ng.cls, nl, h->stream));
   CU(h, cudaStreamSynchronize(h->stream));
+  if (h->f[0] && (nl.pitch != h->L.pitch || nl.plane != h->L.plane)) free_pops(h);
   free_grid(h->g);
   h->g = ng;
+  h->L = nl;
   ng = DevGrid();
   h->have_grid = true;
   h->dx = dx;
@@ -243,6 +295,7 @@ int aerosim_create(int device, aerosim_engine** out) {
   h->device = device;
   default_config(&h->cfg);
   e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
@@ -448,32 +501,32 @@ int aerosim_step(aerosim_engine* h, int32_t n) {
   a.cls = g.cls; a.bmap = g.bmap; a.q = g.q;
   a.mux = h->mux; a.muy = h->muy; a.muz = h->muz; a.mrho = h->mrho;
   a.abl = h->abl; a.sin_tab = h->sin_tab; a.st = h->st;
-  a.stride = h->stride; a.fluid_count = h->fluid_count;
-  a.nx = g.nx; a.ny = g.ny; a.nz = g.nz;
+  a.L = h->L; a.fluid_count = h->fluid_count;
+  a.stages = h->stages;
   a.ground_no_slip = h->cfg.ground_no_slip;
   a.u_inlet = h->cfg.u_inlet_lattice;
   a.tau0 = 3.0 * h->cfg.nu_lattice + 0.5;
   const double cs2 = h->cfg.smagorinsky_cs * h->cfg.smagorinsky_cs;
   a.k_smag = 18.0 * M_SQRT2 * cs2;
-  int tx = ((g.nx + 31) / 32) * 32;
-  if (tx > 256) tx = 256;
-  const int ry = 256 / tx;
   CU(h, cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < n; ++s) {
     a.fsrc = h->f[h->cur];
     a.fdst = h->f[h->cur ^ 1];
     a.step_index = (int)h->step_index;
     a.write_macro = (s == n - 1) ? 1 : 0;
-    CU(h, launch_step(h->cfg.precision, a, tx, ry, h->stream));
+    CU(h, launch_step(h->cfg.precision, a, h->block, h->grid, h->smem, h->stream, nullptr));
     h->cur ^= 1;
     h->step_index += 1;
   }
   CU(h, cudaEventRecord(h->ev1, h->stream));
+  int dev_err = 0;
+  CU(h, cudaMemcpyAsync(&dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(h, cudaStreamSynchronize(h->stream));
   float ms = 0.f;
   CU(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->last_ms = ms;
   h->last_launches = n;
+  if (dev_err) return fail(h, AEROSIM_ERR_DEVICE, "step: the shared-memory pipeline timed out (device error flag set)");
   return AEROSIM_OK;
 }
 
@@ -493,8 +546,7 @@ int aerosim_read_forces(aerosim_engine* h, aerosim_forces* out) {
     a.f = h->f[h->cur];
     a.cls = h->g.cls; a.bcells = h->g.bcells; a.q = h->g.q; a.st = h->st;
     a.partials = h->force_partials; a.ticket = h->force_ticket; a.out = h->force_out;
-    a.stride = h->stride; a.B = h->g.B;
-    a.nx = h->g.nx; a.ny = h->g.ny; a.nz = h->g.nz;
+    a.L = h->L; a.B = h->g.B;
     a.prev_slot = prev_slot(h);
     const unsigned grid = (unsigned)((h->g.B + 255) / 256);
     CU(h, launch_forces(h->cfg.precision, a, grid, h->stream));
@@ -521,7 +573,7 @@ int aerosim_read_macro(aerosim_engine* h, float* ux, float* uy, float* uz, float
   if (rho) {
     int rc = ensure_staging(h, N * 4);
     if (rc) return rc;
-    CU(h, launch_read_macro(h->mrho, h->g.cls, h->st, prev_slot(h), N, (float*)h->staging, h->stream));
+    CU(h, launch_read_macro(h->mrho, h->g.cls, h->st, prev_slot(h), h->L, N, (float*)h->staging, h->stream));
     CU(h, cudaMemcpyAsync(rho, h->staging, N * 4, cudaMemcpyDeviceToHost, h->stream));
   }
   CU(h, cudaStreamSynchronize(h->stream));
@@ -537,7 +589,7 @@ int aerosim_read_populations(aerosim_engine* h, void* f, int32_t dtype) {
   const size_t bytes = (size_t)19 * N * (dtype == AEROSIM_DTYPE_F32 ? 4 : 8);
   int rc = ensure_staging(h, bytes);
   if (rc) return rc;
-  CU(h, launch_read_pops(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->stride, N, h->staging,
+  CU(h, launch_read_pops(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->L, N, h->staging,
                          dtype, h->stream));
   CU(h, cudaMemcpyAsync(f, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
   CU(h, cudaStreamSynchronize(h->stream));
@@ -554,7 +606,7 @@ int aerosim_write_populations(aerosim_engine* h, const void* f, int32_t dtype) {
   int rc = ensure_staging(h, bytes);
   if (rc) return rc;
   CU(h, cudaMemcpyAsync(h->staging, f, bytes, cudaMemcpyHostToDevice, h->stream));
-  CU(h, launch_write_pops(h->f_prec, h->f[h->cur], h->stride, N, h->staging, dtype, h->stream));
+  CU(h, launch_write_pops(h->f_prec, h->f[h->cur], h->L, N, h->staging, dtype, h->stream));
   // the written values are final: no rescale is pending on them
   StepState s{};
   CU(h, cudaMemcpyAsync(&s, h->st, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
@@ -572,7 +624,7 @@ int aerosim_mass_stats(aerosim_engine* h, aerosim_mass* out) {
   unsigned long long r[4];
   StepState s{};
   CU(h, cudaMemsetAsync(h->stats_buf, 0, sizeof(r), h->stream));
-  CU(h, launch_mass_stats(h->mux, h->muy, h->muz, h->mrho, h->g.cls, h->st, prev_slot(h), h->g.N,
+  CU(h, launch_mass_stats(h->mux, h->muy, h->muz, h->mrho, h->g.cls, h->st, prev_slot(h), h->L, h->g.N,
                           h->stats_buf, h->stream));
   CU(h, cudaMemcpyAsync(r, h->stats_buf, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
   CU(h, cudaMemcpyAsync(&s, h->st, sizeof(s), cudaMemcpyDeviceToHost, h->stream));

@@ -3,12 +3,12 @@
 #include <cstdint>
 #include <string>
 #include <cuda_runtime.h>
+#include "common.cuh"
 
 namespace aerosim {
 
 struct StepArgs;
 struct ForceArgs;
-struct StepState;
 
 // A voxel grid resident on the device (VoxelGridResult, voxelizer.ts:19-59).
 struct DevGrid {
@@ -35,23 +35,26 @@ int run_voxelizer(const float* pos, int64_t nverts, const int32_t* idx, int64_t 
 size_t precision_bytes(int precision);
 
 // lbm_fast.cu / lbm_exact.cu
-cudaError_t launch_step(int precision, const StepArgs& a, int tx, int ry, cudaStream_t s);
+// occ != nullptr: only query the resident CTAs per SM (and raise the shared-memory
+// attribute) for this block and dynamic shared-memory size.
+cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s,
+                        int* occ);
 cudaError_t launch_forces(int precision, const ForceArgs& a, unsigned grid, cudaStream_t s);
-cudaError_t launch_classify(const uint8_t* flags, uint8_t* cls, int nx, int ny, int nz, cudaStream_t s);
+cudaError_t launch_classify(const uint8_t* flags, uint8_t* cls, const Layout& L, cudaStream_t s);
 cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, float* mux, float* muy,
-                        float* muz, float* mrho, const double* abl, long long stride, int nx, int ny,
-                        int nz, double u_inlet, int ground_no_slip, cudaStream_t s);
+                        float* muz, float* mrho, const double* abl, const Layout& L, double u_inlet,
+                        int ground_no_slip, cudaStream_t s);
 cudaError_t launch_read_pops(int precision, const void* f, const uint8_t* cls, const StepState* st,
-                             int prev_slot, long long stride, long long N, void* out, int dtype,
+                             int prev_slot, const Layout& L, long long N, void* out, int dtype,
                              cudaStream_t s);
-cudaError_t launch_write_pops(int precision, void* f, long long stride, long long N, const void* in,
+cudaError_t launch_write_pops(int precision, void* f, const Layout& L, long long N, const void* in,
                               int dtype, cudaStream_t s);
 cudaError_t launch_materialize(int precision, void* f, const uint8_t* cls, const StepState* st,
-                               int prev_slot, long long stride, long long N, cudaStream_t s);
+                               int prev_slot, const Layout& L, long long N, cudaStream_t s);
 cudaError_t launch_read_macro(const float* mrho, const uint8_t* cls, const StepState* st, int prev_slot,
-                              long long N, float* rho_out, cudaStream_t s);
+                              const Layout& L, long long N, float* rho_out, cudaStream_t s);
 cudaError_t launch_mass_stats(const float* mux, const float* muy, const float* muz, const float* rho,
-                              const uint8_t* cls, const StepState* st, int prev_slot, long long N,
-                              unsigned long long* out, cudaStream_t s);
+                              const uint8_t* cls, const StepState* st, int prev_slot, const Layout& L,
+                              long long N, unsigned long long* out, cudaStream_t s);
 
 }  // namespace aerosim

@@ -9,7 +9,8 @@ namespace aerosim {
 // Cell classes from the reference flags: CLS_NEAR marks non-solid cells for which
 // some clamped pull source clamp(x - c_d), d >= 1, is SOLID (lbmCpuReference.ts:190-196).
 __global__ void classify_kernel(const uint8_t* __restrict__ flags, uint8_t* __restrict__ cls,
-                                int nx, int ny, int nz) {
+                                const Layout L) {
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
   const long long N = (long long)nx * ny * nz;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
@@ -29,7 +30,7 @@ __global__ void classify_kernel(const uint8_t* __restrict__ flags, uint8_t* __re
       }
       if (near) c |= CLS_NEAR;
     }
-    cls[i] = c;
+    cls[L.cls_at(i)] = c;
   }
 }
 
@@ -37,12 +38,13 @@ __global__ void classify_kernel(const uint8_t* __restrict__ flags, uint8_t* __re
 // inlet speed (ABL profile when groundNoSlip, 0 at iy = 0) and 0 inside solids.
 template <class S>
 __global__ void init_kernel(void* f0, void* f1, const uint8_t* __restrict__ cls, float* mux,
-                            float* muy, float* muz, float* mrho, const double* abl, long long stride,
-                            int nx, int ny, int nz, double u_inlet, int ground_no_slip) {
+                            float* muy, float* muz, float* mrho, const double* abl, const Layout L,
+                            double u_inlet, int ground_no_slip) {
   using T = typename S::T;
   T* a = static_cast<T*>(f0);
   T* b = static_cast<T*>(f1);
-  const long long N = (long long)nx * ny * nz;
+  const int nx = L.nx, ny = L.ny;
+  const long long N = (long long)nx * ny * L.nz;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
     const int iy = (int)((i / nx) % ny);
@@ -51,13 +53,13 @@ __global__ void init_kernel(void* f0, void* f1, const uint8_t* __restrict__ cls,
       u0 = u_inlet * abl[iy];
       if (iy == 0) u0 = 0;
     }
-    if ((cls[i] & CLS_FLAG_MASK) == CELL_SOLID) u0 = 0.0;
+    if ((cls[L.cls_at(i)] & CLS_FLAG_MASK) == CELL_SOLID) u0 = 0.0;
     mux[i] = (float)u0; muy[i] = 0.0f; muz[i] = 0.0f; mrho[i] = 1.0f;
 #pragma unroll
     for (int d = 0; d < 19; ++d) {
       const T e = S::raw_of_f(feq64(d, 1.0, u0, 0.0, 0.0), d);
-      a[d * stride + i] = e;
-      b[d * stride + i] = e;
+      a[L.at(d, i)] = e;
+      b[L.at(d, i)] = e;
     }
   }
 }
@@ -66,7 +68,7 @@ __global__ void init_kernel(void* f0, void* f1, const uint8_t* __restrict__ cls,
 // cells, exactly as the reference's Float32Array holds them after the rescale.
 template <class S, int MODE, class Out>
 __global__ void read_pops_kernel(const void* f, const uint8_t* __restrict__ cls,
-                                 const StepState* st, int prev_slot, long long stride, long long N,
+                                 const StepState* st, int prev_slot, const Layout L, long long N,
                                  Out* __restrict__ out) {
   using T = typename S::T;
   const T* src = static_cast<const T*>(f);
@@ -74,10 +76,10 @@ __global__ void read_pops_kernel(const void* f, const uint8_t* __restrict__ cls,
   const double corr = apply ? st->corr[prev_slot] : 1.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
-    const bool solid = (cls[i] & CLS_FLAG_MASK) == CELL_SOLID;
+    const bool solid = (cls[L.cls_at(i)] & CLS_FLAG_MASK) == CELL_SOLID;
 #pragma unroll
     for (int d = 0; d < 19; ++d) {
-      double v = S::f_of(src[d * stride + i], d);
+      double v = S::f_of(src[L.at(d, i)], d);
       if (!solid && apply) {
         v = v * corr;
         if constexpr (MODE == MODE_MIRROR) v = (double)(float)v;
@@ -88,13 +90,13 @@ __global__ void read_pops_kernel(const void* f, const uint8_t* __restrict__ cls,
 }
 
 template <class S, class In>
-__global__ void write_pops_kernel(void* f, long long stride, long long N, const In* __restrict__ in) {
+__global__ void write_pops_kernel(void* f, const Layout L, long long N, const In* __restrict__ in) {
   using T = typename S::T;
   T* dst = static_cast<T*>(f);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
 #pragma unroll
-    for (int d = 0; d < 19; ++d) dst[d * stride + i] = S::raw_of_f((double)in[d * N + i], d);
+    for (int d = 0; d < 19; ++d) dst[L.at(d, i)] = S::raw_of_f((double)in[d * N + i], d);
   }
 }
 
@@ -102,7 +104,7 @@ __global__ void write_pops_kernel(void* f, long long stride, long long N, const 
 // flow reset, so the correction is not later applied with the new flags).
 template <class S, int MODE>
 __global__ void materialize_rescale_kernel(void* f, const uint8_t* __restrict__ cls,
-                                           const StepState* st, int prev_slot, long long stride,
+                                           const StepState* st, int prev_slot, const Layout L,
                                            long long N) {
   using T = typename S::T;
   T* dst = static_cast<T*>(f);
@@ -111,23 +113,22 @@ __global__ void materialize_rescale_kernel(void* f, const uint8_t* __restrict__ 
   const double corr = st->corr[prev_slot];
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
-    if ((cls[i] & CLS_FLAG_MASK) == CELL_SOLID) continue;
+    if ((cls[L.cls_at(i)] & CLS_FLAG_MASK) == CELL_SOLID) continue;
 #pragma unroll
-    for (int d = 0; d < 19; ++d)
-      dst[d * stride + i] = S::raw_of_f(S::f_of(dst[d * stride + i], d) * corr, d);
+    for (int d = 0; d < 19; ++d) dst[L.at(d, i)] = S::raw_of_f(S::f_of(dst[L.at(d, i)], d) * corr, d);
   }
 }
 
 // Macro readback with the pending rescale on rho (rho[idx] *= corr, :448).
 __global__ void read_macro_kernel(const float* __restrict__ mrho, const uint8_t* __restrict__ cls,
-                                  const StepState* st, int prev_slot, long long N,
+                                  const StepState* st, int prev_slot, const Layout L, long long N,
                                   float* __restrict__ rho_out) {
   const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
   const double corr = apply ? st->corr[prev_slot] : 1.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
     float r = mrho[i];
-    if (apply && (cls[i] & CLS_FLAG_MASK) != CELL_SOLID) r = (float)((double)r * corr);
+    if (apply && (cls[L.cls_at(i)] & CLS_FLAG_MASK) != CELL_SOLID) r = (float)((double)r * corr);
     rho_out[i] = r;
   }
 }
@@ -139,7 +140,7 @@ __global__ void read_macro_kernel(const float* __restrict__ mrho, const uint8_t*
 __global__ void mass_stats_kernel(const float* __restrict__ mux, const float* __restrict__ muy,
                                   const float* __restrict__ muz, const float* __restrict__ rho,
                                   const uint8_t* __restrict__ cls, const StepState* st,
-                                  int prev_slot, long long N, unsigned long long* out) {
+                                  int prev_slot, const Layout L, long long N, unsigned long long* out) {
   const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
   const double corr = apply ? st->corr[prev_slot] : 1.0;
   long long s = 0, cnt = 0;
@@ -147,7 +148,7 @@ __global__ void mass_stats_kernel(const float* __restrict__ mux, const float* __
   int nan = 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
-    if ((cls[i] & CLS_FLAG_MASK) == CELL_SOLID) continue;
+    if ((cls[L.cls_at(i)] & CLS_FLAG_MASK) == CELL_SOLID) continue;
     float r = rho[i];
     if (apply) r = (float)((double)r * corr);
     const float u = mux[i], v = muy[i], w = muz[i];

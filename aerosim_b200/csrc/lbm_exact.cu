@@ -5,13 +5,14 @@
 #include <type_traits>
 #include "common.cuh"
 #include "engine_internal.h"
-#include "lbm_kernels.cuh"
+#include "lbm_launch.cuh"
 #include "lbm_aux.cuh"
 #include "../../include/aerosim.h"
 
 namespace aerosim {
 
-cudaError_t launch_step_fast(int precision, const StepArgs& a, int tx, int ry, cudaStream_t s);
+cudaError_t launch_step_fast(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
+                             cudaStream_t s, int* occ);
 
 size_t precision_bytes(int precision) {
   switch (precision) {
@@ -22,26 +23,12 @@ size_t precision_bytes(int precision) {
   }
 }
 
-template <class S, int MODE>
-static cudaError_t step_dbl(const StepArgs& a, int tx, int ry, cudaStream_t s) {
-  const long long rows = (long long)a.ny * a.nz;
-  const unsigned grid = (unsigned)((rows + ry - 1) / ry);
-  const dim3 block(tx, ry);
-  switch (ry) {
-    case 1: step_kernel<S, MODE, 1><<<grid, block, 0, s>>>(a); break;
-    case 2: step_kernel<S, MODE, 2><<<grid, block, 0, s>>>(a); break;
-    case 4: step_kernel<S, MODE, 4><<<grid, block, 0, s>>>(a); break;
-    case 8: step_kernel<S, MODE, 8><<<grid, block, 0, s>>>(a); break;
-    default: return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t launch_step(int precision, const StepArgs& a, int tx, int ry, cudaStream_t s) {
+cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
+                        cudaStream_t s, int* occ) {
   switch (precision) {
-    case AEROSIM_PREC_F32_MIRROR: return step_dbl<StoreF32, MODE_MIRROR>(a, tx, ry, s);
-    case AEROSIM_PREC_F64: return step_dbl<StoreF64, MODE_F64>(a, tx, ry, s);
-    default: return launch_step_fast(precision, a, tx, ry, s);
+    case AEROSIM_PREC_F32_MIRROR: return step_entry<StoreF32, MODE_MIRROR>(a, block, grid, smem, s, occ);
+    case AEROSIM_PREC_F64: return step_entry<StoreF64, MODE_F64>(a, block, grid, smem, s, occ);
+    default: return launch_step_fast(precision, a, block, grid, smem, s, occ);
   }
 }
 
@@ -63,16 +50,16 @@ static unsigned grid_for(long long n) {
   return (unsigned)(g < 1 ? 1 : g);
 }
 
-cudaError_t launch_classify(const uint8_t* flags, uint8_t* cls, int nx, int ny, int nz, cudaStream_t s) {
-  classify_kernel<<<grid_for((long long)nx * ny * nz), 256, 0, s>>>(flags, cls, nx, ny, nz);
+cudaError_t launch_classify(const uint8_t* flags, uint8_t* cls, const Layout& L, cudaStream_t s) {
+  classify_kernel<<<grid_for((long long)L.nx * L.ny * L.nz), 256, 0, s>>>(flags, cls, L);
   return cudaGetLastError();
 }
 
 cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, float* mux, float* muy,
-                        float* muz, float* mrho, const double* abl, long long stride, int nx, int ny,
-                        int nz, double u_inlet, int gns, cudaStream_t s) {
-  const unsigned g = grid_for((long long)nx * ny * nz);
-#define AEROSIM_INIT(S) init_kernel<S><<<g, 256, 0, s>>>(f0, f1, cls, mux, muy, muz, mrho, abl, stride, nx, ny, nz, u_inlet, gns)
+                        float* muz, float* mrho, const double* abl, const Layout& L, double u_inlet, int gns,
+                        cudaStream_t s) {
+  const unsigned g = grid_for((long long)L.nx * L.ny * L.nz);
+#define AEROSIM_INIT(S) init_kernel<S><<<g, 256, 0, s>>>(f0, f1, cls, mux, muy, muz, mrho, abl, L, u_inlet, gns)
   switch (precision) {
     case AEROSIM_PREC_F32: case AEROSIM_PREC_F32_MIRROR: AEROSIM_INIT(StoreF32); break;
     case AEROSIM_PREC_F16S: AEROSIM_INIT(StoreF16S); break;
@@ -85,71 +72,71 @@ cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, f
 }
 
 template <class S, int MODE>
-static void read_pops_t(const void* f, const uint8_t* cls, const StepState* st, int ps, long long stride,
+static void read_pops_t(const void* f, const uint8_t* cls, const StepState* st, int ps, const Layout& L,
                         long long N, void* out, int dtype, cudaStream_t s) {
   if (dtype == AEROSIM_DTYPE_F32)
-    read_pops_kernel<S, MODE, float><<<grid_for(N), 256, 0, s>>>(f, cls, st, ps, stride, N, (float*)out);
+    read_pops_kernel<S, MODE, float><<<grid_for(N), 256, 0, s>>>(f, cls, st, ps, L, N, (float*)out);
   else
-    read_pops_kernel<S, MODE, double><<<grid_for(N), 256, 0, s>>>(f, cls, st, ps, stride, N, (double*)out);
+    read_pops_kernel<S, MODE, double><<<grid_for(N), 256, 0, s>>>(f, cls, st, ps, L, N, (double*)out);
 }
 
 cudaError_t launch_read_pops(int precision, const void* f, const uint8_t* cls, const StepState* st,
-                             int ps, long long stride, long long N, void* out, int dtype, cudaStream_t s) {
+                             int ps, const Layout& L, long long N, void* out, int dtype, cudaStream_t s) {
   switch (precision) {
-    case AEROSIM_PREC_F32: read_pops_t<StoreF32, MODE_FAST>(f, cls, st, ps, stride, N, out, dtype, s); break;
-    case AEROSIM_PREC_F32_MIRROR: read_pops_t<StoreF32, MODE_MIRROR>(f, cls, st, ps, stride, N, out, dtype, s); break;
-    case AEROSIM_PREC_F16S: read_pops_t<StoreF16S, MODE_FAST>(f, cls, st, ps, stride, N, out, dtype, s); break;
-    case AEROSIM_PREC_BF16S: read_pops_t<StoreBF16S, MODE_FAST>(f, cls, st, ps, stride, N, out, dtype, s); break;
-    case AEROSIM_PREC_F64: read_pops_t<StoreF64, MODE_F64>(f, cls, st, ps, stride, N, out, dtype, s); break;
+    case AEROSIM_PREC_F32: read_pops_t<StoreF32, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
+    case AEROSIM_PREC_F32_MIRROR: read_pops_t<StoreF32, MODE_MIRROR>(f, cls, st, ps, L, N, out, dtype, s); break;
+    case AEROSIM_PREC_F16S: read_pops_t<StoreF16S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
+    case AEROSIM_PREC_BF16S: read_pops_t<StoreBF16S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
+    case AEROSIM_PREC_F64: read_pops_t<StoreF64, MODE_F64>(f, cls, st, ps, L, N, out, dtype, s); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
 template <class S>
-static void write_pops_t(void* f, long long stride, long long N, const void* in, int dtype, cudaStream_t s) {
+static void write_pops_t(void* f, const Layout& L, long long N, const void* in, int dtype, cudaStream_t s) {
   if (dtype == AEROSIM_DTYPE_F32)
-    write_pops_kernel<S, float><<<grid_for(N), 256, 0, s>>>(f, stride, N, (const float*)in);
+    write_pops_kernel<S, float><<<grid_for(N), 256, 0, s>>>(f, L, N, (const float*)in);
   else
-    write_pops_kernel<S, double><<<grid_for(N), 256, 0, s>>>(f, stride, N, (const double*)in);
+    write_pops_kernel<S, double><<<grid_for(N), 256, 0, s>>>(f, L, N, (const double*)in);
 }
 
-cudaError_t launch_write_pops(int precision, void* f, long long stride, long long N, const void* in,
+cudaError_t launch_write_pops(int precision, void* f, const Layout& L, long long N, const void* in,
                               int dtype, cudaStream_t s) {
   switch (precision) {
-    case AEROSIM_PREC_F32: case AEROSIM_PREC_F32_MIRROR: write_pops_t<StoreF32>(f, stride, N, in, dtype, s); break;
-    case AEROSIM_PREC_F16S: write_pops_t<StoreF16S>(f, stride, N, in, dtype, s); break;
-    case AEROSIM_PREC_BF16S: write_pops_t<StoreBF16S>(f, stride, N, in, dtype, s); break;
-    case AEROSIM_PREC_F64: write_pops_t<StoreF64>(f, stride, N, in, dtype, s); break;
+    case AEROSIM_PREC_F32: case AEROSIM_PREC_F32_MIRROR: write_pops_t<StoreF32>(f, L, N, in, dtype, s); break;
+    case AEROSIM_PREC_F16S: write_pops_t<StoreF16S>(f, L, N, in, dtype, s); break;
+    case AEROSIM_PREC_BF16S: write_pops_t<StoreBF16S>(f, L, N, in, dtype, s); break;
+    case AEROSIM_PREC_F64: write_pops_t<StoreF64>(f, L, N, in, dtype, s); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_materialize(int precision, void* f, const uint8_t* cls, const StepState* st, int ps,
-                               long long stride, long long N, cudaStream_t s) {
+                               const Layout& L, long long N, cudaStream_t s) {
   const unsigned g = grid_for(N);
   switch (precision) {
-    case AEROSIM_PREC_F32: materialize_rescale_kernel<StoreF32, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, stride, N); break;
-    case AEROSIM_PREC_F32_MIRROR: materialize_rescale_kernel<StoreF32, MODE_MIRROR><<<g, 256, 0, s>>>(f, cls, st, ps, stride, N); break;
-    case AEROSIM_PREC_F16S: materialize_rescale_kernel<StoreF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, stride, N); break;
-    case AEROSIM_PREC_BF16S: materialize_rescale_kernel<StoreBF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, stride, N); break;
-    case AEROSIM_PREC_F64: materialize_rescale_kernel<StoreF64, MODE_F64><<<g, 256, 0, s>>>(f, cls, st, ps, stride, N); break;
+    case AEROSIM_PREC_F32: materialize_rescale_kernel<StoreF32, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
+    case AEROSIM_PREC_F32_MIRROR: materialize_rescale_kernel<StoreF32, MODE_MIRROR><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
+    case AEROSIM_PREC_F16S: materialize_rescale_kernel<StoreF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
+    case AEROSIM_PREC_BF16S: materialize_rescale_kernel<StoreBF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
+    case AEROSIM_PREC_F64: materialize_rescale_kernel<StoreF64, MODE_F64><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_read_macro(const float* mrho, const uint8_t* cls, const StepState* st, int ps, long long N,
-                              float* rho_out, cudaStream_t s) {
-  read_macro_kernel<<<grid_for(N), 256, 0, s>>>(mrho, cls, st, ps, N, rho_out);
+cudaError_t launch_read_macro(const float* mrho, const uint8_t* cls, const StepState* st, int ps,
+                              const Layout& L, long long N, float* rho_out, cudaStream_t s) {
+  read_macro_kernel<<<grid_for(N), 256, 0, s>>>(mrho, cls, st, ps, L, N, rho_out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mass_stats(const float* mux, const float* muy, const float* muz, const float* rho,
-                              const uint8_t* cls, const StepState* st, int ps, long long N,
+                              const uint8_t* cls, const StepState* st, int ps, const Layout& L, long long N,
                               unsigned long long* out, cudaStream_t s) {
-  mass_stats_kernel<<<grid_for(N), 256, 0, s>>>(mux, muy, muz, rho, cls, st, ps, N, out);
+  mass_stats_kernel<<<grid_for(N), 256, 0, s>>>(mux, muy, muz, rho, cls, st, ps, L, N, out);
   return cudaGetLastError();
 }
 

@@ -4,31 +4,17 @@
 #include <type_traits>
 #include "common.cuh"
 #include "engine_internal.h"
-#include "lbm_kernels.cuh"
+#include "lbm_launch.cuh"
 #include "../../include/aerosim.h"
 
 namespace aerosim {
 
-template <class S>
-static cudaError_t step_fast(const StepArgs& a, int tx, int ry, cudaStream_t s) {
-  const long long rows = (long long)a.ny * a.nz;
-  const unsigned grid = (unsigned)((rows + ry - 1) / ry);
-  const dim3 block(tx, ry);
-  switch (ry) {
-    case 1: step_kernel<S, MODE_FAST, 1><<<grid, block, 0, s>>>(a); break;
-    case 2: step_kernel<S, MODE_FAST, 2><<<grid, block, 0, s>>>(a); break;
-    case 4: step_kernel<S, MODE_FAST, 4><<<grid, block, 0, s>>>(a); break;
-    case 8: step_kernel<S, MODE_FAST, 8><<<grid, block, 0, s>>>(a); break;
-    default: return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t launch_step_fast(int precision, const StepArgs& a, int tx, int ry, cudaStream_t s) {
+cudaError_t launch_step_fast(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
+                             cudaStream_t s, int* occ) {
   switch (precision) {
-    case AEROSIM_PREC_F32: return step_fast<StoreF32>(a, tx, ry, s);
-    case AEROSIM_PREC_F16S: return step_fast<StoreF16S>(a, tx, ry, s);
-    case AEROSIM_PREC_BF16S: return step_fast<StoreBF16S>(a, tx, ry, s);
+    case AEROSIM_PREC_F32: return step_entry<StoreF32, MODE_FAST>(a, block, grid, smem, s, occ);
+    case AEROSIM_PREC_F16S: return step_entry<StoreF16S, MODE_FAST>(a, block, grid, smem, s, occ);
+    case AEROSIM_PREC_BF16S: return step_entry<StoreBF16S, MODE_FAST>(a, block, grid, smem, s, occ);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -24,22 +24,27 @@ namespace aerosim {
 
 enum { MODE_FAST = 0, MODE_MIRROR = 1, MODE_F64 = 2 };
 
+// Resident CTAs per SM the FP32 step kernel is register-budgeted for.
+#ifndef AEROSIM_FAST_MIN_BLOCKS
+#define AEROSIM_FAST_MIN_BLOCKS 2
+#endif
+
 struct StepArgs {
   const void* fsrc;
   void* fdst;
-  const uint8_t* cls;
-  const int32_t* bmap;
+  const uint8_t* cls;     // pitched cell classes
+  const int32_t* bmap;    // dense boundaryIndexMap
   const float* q;
-  float* mux;
+  float* mux;             // dense macro outputs
   float* muy;
   float* muz;
   float* mrho;
   const double* abl;      // [ny] Math.min(1.15, 0.35 + 0.8 * yFrac^0.3)
   const double* sin_tab;  // [120 * ny] sin(step * 0.15 + (iy / ny) * PI * 2)
   StepState* st;
-  long long stride;       // elements between direction planes (>= N)
+  Layout L;
   long long fluid_count;  // non-solid cells
-  int nx, ny, nz;
+  int stages;             // depth of the shared-memory ring
   int step_index;
   int write_macro;
   int ground_no_slip;
@@ -55,9 +60,8 @@ struct ForceArgs {
   double* partials;       // [gridDim.x * 8]
   unsigned int* ticket;
   double* out;            // [8]: fx fy fz mx my mz cut_face_links blocks
-  long long stride;
+  Layout L;
   long long B;
-  int nx, ny, nz;
   int prev_slot;          // state slot of the step that produced f (-1: none)
 };
 
@@ -68,7 +72,7 @@ struct MacroOf<double> { using type = double; };
 
 // Fixed-point weight of a density in the rescale sum.  A float density in
 // [0.25, 2) is an exact multiple of 2^-25; double densities use 2^-36.
-__device__ __forceinline__ long long rho_fixed(float r) { return llrint((double)r * 33554432.0); }
+__device__ __forceinline__ long long rho_fixed(float r) { return (long long)__float2int_rn(r * 33554432.0f); }
 __device__ __forceinline__ long long rho_fixed(double r) { return llrint(r * 68719476736.0); }
 __device__ __forceinline__ double rho_unfixed(long long s, float) { return (double)s * (1.0 / 33554432.0); }
 __device__ __forceinline__ double rho_unfixed(long long s, double) { return (double)s * (1.0 / 68719476736.0); }
@@ -81,14 +85,38 @@ __device__ __forceinline__ double feq64(int d, double rho, double ux, double uy,
   return w64_of(d) * rho * (1.0 + cu + 0.5 * cu * cu - 1.5 * uSq);
 }
 
+// c_d . u with the zero components left out (d is a constant after unrolling).
+__device__ __forceinline__ float dotc(int d, float x, float y, float z) {
+  const int a = cx_of(d), b = cy_of(d), c = cz_of(d);
+  float s = a ? (a > 0 ? x : -x) : (b ? (b > 0 ? y : -y) : (c ? (c > 0 ? z : -z) : 0.0f));
+  if (a && b) s += b > 0 ? y : -y;
+  if ((a || b) && c) s += c > 0 ? z : -z;
+  return s;
+}
+
 // FP32 equilibrium deviation feq_d - w_d for the fast path.
 __device__ __forceinline__ float heq32(int d, float rho, float ux, float uy, float uz) {
-  const float cu = 3.0f * ((float)cx_of(d) * ux + (float)cy_of(d) * uy + (float)cz_of(d) * uz);
+  const float cu = 3.0f * dotc(d, ux, uy, uz);
   const float uSq = ux * ux + uy * uy + uz * uz;
   return wf_of(d) * ((rho - 1.0f) + rho * (cu + 0.5f * cu * cu - 1.5f * uSq));
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Runtime-direction lattice tables for loops that are deliberately not unrolled.
+__device__ __forceinline__ int cx_rt(int d) { return cx_of(d); }
+__device__ __forceinline__ int cy_rt(int d) { return cy_of(d); }
+__device__ __forceinline__ int cz_rt(int d) { return cz_of(d); }
+__device__ __forceinline__ double w32_of_rt(int d) { return w32_of(d); }
+// Writes v[d] for a runtime d without forcing the array into local memory.
+template <class R>
+__device__ __forceinline__ void set_rt(R (&v)[19], int d, R x) {
+#pragma unroll
+  for (int k = 0; k < 19; ++k)
+    if (k == d) v[k] = x;
+}
+// The inlet reads rho at ix = 1, which is 1 for a solid cell (:177).
+__device__ __forceinline__ bool solid_at_one(int ix, bool solid) { return ix == 1 && solid; }
 
 // ---------------------------------------------------------------------------
 // Collision kernels for one cell.  In: pulled values v[19] (already rescaled).
@@ -104,13 +132,15 @@ __device__ __forceinline__ void collide_f64(double (&v)[19], double& r, double& 
                                             double& uz, double tau0, double k_smag) {
   double fl[19];
   r = 0.0; ux = 0.0; uy = 0.0; uz = 0.0;
+  // Terms with a zero lattice component only add a signed zero to these sums, which
+  // leaves every value the reference can produce unchanged, so they are skipped.
 #pragma unroll
   for (int d = 0; d < 19; ++d) {
     fl[d] = MIRROR ? (double)(float)v[d] : v[d];
     r += v[d];
-    ux += (double)cx_of(d) * v[d];
-    uy += (double)cy_of(d) * v[d];
-    uz += (double)cz_of(d) * v[d];
+    if (cx_of(d)) ux += (double)cx_of(d) * v[d];
+    if (cy_of(d)) uy += (double)cy_of(d) * v[d];
+    if (cz_of(d)) uz += (double)cz_of(d) * v[d];
   }
   r = js_max(0.5, js_min(1.8, r));
   const double ir = 1.0 / r;
@@ -130,12 +160,12 @@ __device__ __forceinline__ void collide_f64(double (&v)[19], double& r, double& 
     const double eq = w32_of(d) * r * (1.0 + cu + 0.5 * cu * cu - 1.5 * uSq);
     fe[d] = MIRROR ? (double)(float)eq : eq;
     const double fn = fl[d] - eq;
-    pxx += cx * cx * fn;
-    pyy += cy * cy * fn;
-    pzz += cz * cz * fn;
-    pxy += cx * cy * fn;
-    pxz += cx * cz * fn;
-    pyz += cy * cz * fn;
+    if (cx_of(d)) pxx += cx * cx * fn;
+    if (cy_of(d)) pyy += cy * cy * fn;
+    if (cz_of(d)) pzz += cz * cz * fn;
+    if (cx_of(d) * cy_of(d)) pxy += cx * cy * fn;
+    if (cx_of(d) * cz_of(d)) pxz += cx * cz * fn;
+    if (cy_of(d) * cz_of(d)) pyz += cy * cz * fn;
   }
   const double pn = sqrt(pxx * pxx + pyy * pyy + pzz * pzz + 2.0 * (pxy * pxy + pxz * pxz + pyz * pyz));
   const double tau = 0.5 * (tau0 + sqrt(tau0 * tau0 + (k_smag * pn) / r));
@@ -151,295 +181,476 @@ __device__ __forceinline__ void collide_f64(double (&v)[19], double& r, double& 
   }
 }
 
-// FP32 path.  Works on deviations h_d = f_d - w_d: the moments are
-//   rho - 1 = sum h,  j = sum c h,  Pi^neq = sum cc h - (rho - 1)/3 I - rho u u,
-// which equals the reference's sum cc (f - feq) but keeps the small quantities
-// free of the cancellation against w_d.
+// FP32 path on deviations h_d = f_d - w_d, organised by the 9 opposite pairs
+// (2p+1, 2p+2) of D3Q19 so that no multiplication by a zero lattice component is
+// left for the compiler (IEEE semantics forbid folding 0 * x):
+//   pair sums s_p = h_a + h_b give rho - 1 and the second moments,
+//   pair differences t_p = h_a - h_b give the momentum;
+//   Pi^neq = sum cc h - (rho - 1)/3 I - rho u u  (= the reference's sum cc (f - feq));
+//   post-collision h_a,b = E_p +- O_p with the even part
+//   E = w (rho - 1 - 1.5 rho u^2 + 4.5 rho (c.u)^2 + (1 - omega) 4.5 Q:Pi) and the odd
+//   part O = 3 w rho (c.u), Q:Pi = c.Pi.c - tr(Pi) / 3.
+// Pairs: 0 (+-x), 1 (+-y), 2 (+-z), 3 +-(x+y), 4 +-(x-y), 5 +-(x+z), 6 +-(x-z),
+// 7 +-(y+z), 8 +-(y-z), matching lbmConstants.ts:10-32.
+__device__ __forceinline__ float frcp(float x) { return __frcp_rn(x); }
+
 __device__ __forceinline__ void collide_f32(float (&h)[19], float& r, float& ux, float& uy,
                                             float& uz, float tau0, float k_smag) {
-  float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-  float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
+  float s[9], t[9];
 #pragma unroll
-  for (int d = 0; d < 19; ++d) {
-    const float cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
-    dr += h[d];
-    if (cx_of(d)) jx += cx * h[d];
-    if (cy_of(d)) jy += cy * h[d];
-    if (cz_of(d)) jz += cz * h[d];
-    if (cx_of(d)) sxx += h[d];
-    if (cy_of(d)) syy += h[d];
-    if (cz_of(d)) szz += h[d];
-    if (cx_of(d) * cy_of(d)) sxy += cx * cy * h[d];
-    if (cx_of(d) * cz_of(d)) sxz += cx * cz * h[d];
-    if (cy_of(d) * cz_of(d)) syz += cy * cz * h[d];
+  for (int p = 0; p < 9; ++p) {
+    s[p] = h[2 * p + 1] + h[2 * p + 2];
+    t[p] = h[2 * p + 1] - h[2 * p + 2];
   }
+  const float dr = h[0] + ((s[0] + s[1]) + (s[2] + s[3]) + ((s[4] + s[5]) + (s[6] + s[7])) + s[8]);
+  const float jx = (t[0] + t[3]) + (t[4] + t[5]) + t[6];
+  const float jy = (t[1] + t[3]) - t[4] + (t[7] + t[8]);
+  const float jz = (t[2] + t[5]) - t[6] + (t[7] - t[8]);
+  const float sxx = (s[0] + s[3]) + (s[4] + s[5]) + s[6];
+  const float syy = (s[1] + s[3]) + (s[4] + s[7]) + s[8];
+  const float szz = (s[2] + s[5]) + (s[6] + s[7]) + s[8];
+  const float sxy = s[3] - s[4], sxz = s[5] - s[6], syz = s[7] - s[8];
+
   r = fmaxf(0.5f, fminf(1.8f, 1.0f + dr));
-  if (dr != dr) r = dr;  // keep NaN visible like Math.min/Math.max
-  const float ir = 1.0f / r;
+  if (dr != dr) r = dr;  // keep NaN visible like Math.min / Math.max
+  const float ir = frcp(r);
   ux = jx * ir; uy = jy * ir; uz = jz * ir;
-  const float m2 = ux * ux + uy * uy + uz * uz;
-  if (m2 > 0.0484f) {
-    const float s = 0.22f * rsqrtf(m2);
-    ux *= s; uy *= s; uz *= s;
+  float uSq = ux * ux + uy * uy + uz * uz;
+  if (uSq > 0.0484f) {  // Mach limiter |u| <= 0.22
+    const float sc = 0.22f * rsqrtf(uSq);
+    ux *= sc; uy *= sc; uz *= sc;
+    uSq = ux * ux + uy * uy + uz * uz;
   }
   const float drc = r - 1.0f;
-  const float third = 1.0f / 3.0f;
-  const float pxx = sxx - drc * third - r * ux * ux;
-  const float pyy = syy - drc * third - r * uy * uy;
-  const float pzz = szz - drc * third - r * uz * uz;
-  const float pxy = sxy - r * ux * uy;
-  const float pxz = sxz - r * ux * uz;
-  const float pyz = syz - r * uy * uz;
-  const float pn = sqrtf(pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
-  const float tau = 0.5f * (tau0 + sqrtf(tau0 * tau0 + (k_smag * pn) / r));
-  const float om = 1.0f / fmaxf(0.5015f, fminf(1.95f, tau));
-  const float uSq = ux * ux + uy * uy + uz * uz;
-  const float tr3 = (pxx + pyy + pzz) * third;
+  const float d3 = drc * (1.0f / 3.0f);
+  const float rux = r * ux, ruy = r * uy, ruz = r * uz;
+  const float pxx = fmaf(-rux, ux, sxx - d3);
+  const float pyy = fmaf(-ruy, uy, syy - d3);
+  const float pzz = fmaf(-ruz, uz, szz - d3);
+  const float pxy = fmaf(-rux, uy, sxy);
+  const float pxz = fmaf(-rux, uz, sxz);
+  const float pyz = fmaf(-ruy, uz, syz);
+  const float off = pxy * pxy + pxz * pxz + pyz * pyz;
+  const float pn = sqrtf(pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * off);
+  const float tau = 0.5f * (tau0 + sqrtf(fmaf(tau0, tau0, k_smag * pn * ir)));
+  const float om = frcp(fmaxf(0.5015f, fminf(1.95f, tau)));
   const float g = (1.0f - om) * 4.5f;
+  const float tr3 = (pxx + pyy + pzz) * (1.0f / 3.0f);
+  const float A = fmaf(-1.5f * r, uSq, drc);
+  constexpr float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
+  // rest population
+  h[0] = w0 * fmaf(-g, tr3, A);
+  // faces: Q:Pi = P_aa - tr/3
+  const float k1 = w1 * 4.5f * r, o1 = w1 * 3.0f * r, g1 = w1 * g, a1 = w1 * A;
+  const float qx = pxx - tr3, qy = pyy - tr3, qz = pzz - tr3;
+  const float cuf[3] = {ux, uy, uz};
+  const float qf[3] = {qx, qy, qz};
 #pragma unroll
-  for (int d = 0; d < 19; ++d) {
-    const float cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
-    const float cu = 3.0f * (cx * ux + cy * uy + cz * uz);
-    const float heq = wf_of(d) * (drc + r * (cu + 0.5f * cu * cu - 1.5f * uSq));
-    const float qpi = cx * cx * pxx + cy * cy * pyy + cz * cz * pzz +
-                      2.0f * (cx * cy * pxy + cx * cz * pxz + cy * cz * pyz) - tr3;
-    h[d] = heq + g * wf_of(d) * qpi;
+  for (int p = 0; p < 3; ++p) {
+    const float E = fmaf(k1, cuf[p] * cuf[p], fmaf(g1, qf[p], a1));
+    const float O = o1 * cuf[p];
+    h[2 * p + 1] = E + O;
+    h[2 * p + 2] = E - O;
+  }
+  // edges: Q:Pi = P_aa + P_bb - tr/3 +- 2 P_ab
+  const float k2 = w2 * 4.5f * r, o2 = w2 * 3.0f * r, g2 = w2 * g, a2 = w2 * A;
+  const float bxy = pxx + pyy - tr3, bxz = pxx + pzz - tr3, byz = pyy + pzz - tr3;
+  const float cue[6] = {ux + uy, ux - uy, ux + uz, ux - uz, uy + uz, uy - uz};
+  const float qe[6] = {fmaf(2.0f, pxy, bxy), fmaf(-2.0f, pxy, bxy), fmaf(2.0f, pxz, bxz),
+                       fmaf(-2.0f, pxz, bxz), fmaf(2.0f, pyz, byz), fmaf(-2.0f, pyz, byz)};
+#pragma unroll
+  for (int p = 0; p < 6; ++p) {
+    const float E = fmaf(k2, cue[p] * cue[p], fmaf(g2, qe[p], a2));
+    const float O = o2 * cue[p];
+    h[2 * p + 7] = E + O;
+    h[2 * p + 8] = E - O;
   }
 }
 
 // ---------------------------------------------------------------------------
-// The fused step kernel.  blockDim = (TX, RY): TX threads along x, RY rows per CTA.
+// 1-D bulk-copy (TMA) and mbarrier helpers: global -> shared row copies whose
+// completion is counted in bytes on a shared-memory mbarrier.
 // ---------------------------------------------------------------------------
-template <int RY>
-struct RowExchange {
-  double rho1[RY];       // density at ix = 1 (after collision)
-  double fprev[RY][19];  // populations at ix = nx-2 before wall conditions
-  double mprev[RY][4];   // rho, ux, uy, uz at ix = nx-2 before wall conditions
-};
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait: gives up after `limit` polls (each poll suspends the thread briefly).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+constexpr int kWaitLimit = 1 << 22;
+constexpr int kConsumerWarps = 8;
+constexpr int kStepThreads = (kConsumerWarps + 1) * 32;
+enum { STEP_ERR_PIPELINE_TIMEOUT = 1 };
 
-template <class S, int MODE, int RY>
-__global__ void __launch_bounds__(256) step_kernel(const StepArgs a) {
+// Thread -> cell mapping of a row: cell ix = slot - shift with slot = lane + 32 * warp
+// + tx_span * chunk.  shift = 1 when nx = 1 (mod 32) keeps the cell pairs (0, 1) and
+// (nx-2, nx-1) inside one warp, so the inlet and outlet exchange stays warp-local.
+__host__ __device__ inline int row_shift(int nx) { return (nx % 32 == 1) ? 1 : 0; }
+__host__ __device__ inline int row_span(int nx) {  // threads along x (multiple of 32, <= 256)
+  const int t = (nx + row_shift(nx) + 31) / 32 * 32;
+  return t > kConsumerWarps * 32 ? kConsumerWarps * 32 : t;
+}
+__host__ __device__ inline int rows_per_item(int nx) { return (kConsumerWarps * 32) / row_span(nx); }
+
+// Dynamic shared memory of the step kernel: `stages` slots, each holding the 19
+// source row segments and the class bytes of the item's destination rows, plus a
+// full and an empty mbarrier per slot.
+__host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem) {
+  return (size_t)rows_per_item(L.nx) * (19 * (size_t)L.pitch * elem + (size_t)L.pitch);
+}
+// Guard bytes around the slots: the x-face cells read (and discard) one element
+// before the first row or past the end of a row.
+constexpr size_t kSmemGuard = 64;
+__host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem) {
+  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 * (size_t)stages + 16;
+}
+
+// ---------------------------------------------------------------------------
+// The fused step kernel.  Persistent CTAs of 8 consumer warps + 1 producer warp
+// walk the x-rows of the lattice.  The producer issues, per work item, 19 bulk
+// copies per destination row (the clamped source row of every direction plane)
+// plus the class-byte row into a ring of shared-memory slots; a slot's `full`
+// mbarrier completes when its bytes have landed.  Consumer warps own whole row
+// segments: they pull their 19 values from the slot (x-shift by indexing), release
+// the slot on its `empty` mbarrier, collide in registers, settle the inlet / outlet
+// with warp shuffles and store straight to the destination planes.  No CTA-wide
+// barrier is taken inside the row loop.
+// ---------------------------------------------------------------------------
+template <class S, int MODE>
+__global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST_MIN_BLOCKS : 1)
+    step_kernel(const StepArgs a) {
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
   using Mac = typename MacroOf<T>::type;
-  constexpr bool DBL = MODE != MODE_FAST;
 
-  __shared__ RowExchange<RY> ex;
-  __shared__ long long red[32];
-  __shared__ bool is_last;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ long long red[kConsumerWarps + 1];
+  __shared__ int nan_flag;
+  __shared__ int is_last;
+
+  const Layout L = a.L;
+  const int nx = L.nx, ny = L.ny, nz = L.nz, pitch = L.pitch;
+  const long long plane = L.plane;
+  const int S_ = a.stages;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int shift = row_shift(nx), span = row_span(nx), RY = rows_per_item(nx);
+  const int wpr = span / 32;  // warps per row
+  const long long rows = (long long)ny * nz;
+  const long long n_items = (rows + RY - 1) / RY;
+  const int my_count = blockIdx.x < n_items ? (int)((n_items - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+
+  T* spop = reinterpret_cast<T*>(smem_raw + kSmemGuard);
+  uint8_t* scls = smem_raw + kSmemGuard + (size_t)S_ * RY * 19 * pitch * sizeof(T);
+  uint64_t* full = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(scls + (size_t)S_ * RY * pitch + kSmemGuard) + 7) & ~uintptr_t(7));
+  uint64_t* empty = full + S_;
 
   const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
   T* __restrict__ fd = static_cast<T*>(a.fdst);
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const long long rows = (long long)ny * nz;
-  const long long row = (long long)blockIdx.x * RY + ty;
-  const bool row_ok = row < rows;
-  const int iy = row_ok ? (int)(row % ny) : 0;
-  const int iz = row_ok ? (int)(row / ny) : 0;
-  const long long stride = a.stride;
 
-  // Pending rescale of the previous step (slot (step-1)&1; cleared at reset).
-  const int pslot = (a.step_index + 1) & 1;
-  const int apply = a.st->apply[pslot];
-  const double corr = apply ? a.st->corr[pslot] : 1.0;
-  const float corrf = (float)corr;
-
-  // Clamped source row offsets for the 9 (cy, cz) combinations.
-  auto srow = [&](int cy, int cz) -> long long {
-    return (long long)nx * (clampi(iy - cy, 0, ny - 1) + (long long)ny * clampi(iz - cz, 0, nz - 1));
-  };
-  const long long rbase = (long long)nx * (iy + (long long)ny * iz);
-  long long rb[19];
-#pragma unroll
-  for (int d = 0; d < 19; ++d) rb[d] = srow(cy_of(d), cz_of(d));
-  const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S_; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    nan_flag = 0;
+    mbar_fence_init();
+  }
+  __syncthreads();
 
   long long my_sum = 0;
-  int my_nan = 0;
-  const int nchunks = (nx + blockDim.x - 1) / blockDim.x;
-  for (int ch = 0; ch < nchunks; ++ch) {
-    const int ix = ch * blockDim.x + tx;
-    const bool active = row_ok && ix < nx;
-    const long long idx = rbase + ix;
-    const uint8_t c = active ? a.cls[idx] : CELL_SOLID;
-    const int flag = c & CLS_FLAG_MASK;
-    const bool solid = flag == CELL_SOLID;
-    const bool xface = (ix == 0 || ix == nx - 1);
-    Real v[19];
-    Mac mr = (Mac)1, mx = (Mac)0, my = (Mac)0, mz = (Mac)0;
+  bool failed = false;
 
-    if (active && !solid && !xface) {
-      // ---- pull-stream (lbmCpuReference.ts:189-231) ----
-#pragma unroll
-      for (int d = 0; d < 19; ++d) {
-        const T raw = fs[d * stride + rb[d] + ix - cx_of(d)];
-        if constexpr (MODE == MODE_FAST) {
-          float h = S::h_of(raw, d);
-          if (apply) h = h * corrf + wf_of(d) * (corrf - 1.0f);
-          v[d] = h;
-        } else if constexpr (MODE == MODE_MIRROR) {
-          v[d] = (double)(float)(S::f_of(raw, d) * corr);
-        } else {
-          v[d] = S::f_of(raw, d) * corr;
+  if (warp == kConsumerWarps) {
+    // ---------------- producer warp ----------------
+    if (lane == 0) {
+      const uint32_t row_bytes = (uint32_t)(pitch * sizeof(T));
+      int issued = 0;
+      for (int j = 0; j < my_count; ++j) {
+        const int s = j % S_;
+        if (j >= S_ && !mbar_wait(&empty[s], (uint32_t)(((j / S_) - 1) & 1), kWaitLimit)) {
+          failed = true;
+          break;
         }
-      }
-      if (c & CLS_NEAR) {
-        // Bouzidi interpolated bounce-back for solid pull sources (:196-221).
-        const int bi = (flag == CELL_BOUNDARY) ? a.bmap[idx] : -1;
+        const long long r0 = (blockIdx.x + (long long)j * gridDim.x) * RY;
+        const int nr = (int)(rows - r0 < RY ? rows - r0 : RY);
+        mbar_arrive_expect_tx(&full[s], (uint32_t)nr * (19u * row_bytes + (uint32_t)pitch));
+        for (int yy = 0; yy < nr; ++yy) {
+          const long long r = r0 + yy;
+          const int iy = (int)(r % ny), iz = (int)(r / ny);
+          T* dst = spop + ((size_t)s * RY + yy) * 19 * pitch;
 #pragma unroll
-        for (int d = 1; d < 19; ++d) {
-          const long long src = rb[d] + ix - cx_of(d);
-          if ((a.cls[src] & CLS_FLAG_MASK) == CELL_SOLID) {
-            const int wd = opp_of(d);
-            const double qv = bi >= 0 ? (double)a.q[(long long)bi * 18 + (wd - 1)] : 0.5;
-            const double qe = qv > 0.0 ? qv : 0.5;
-            auto popf = [&](int dd, long long i) -> double {
-              const double f = S::f_of(fs[dd * stride + i], dd);
+          for (int d = 0; d < 19; ++d) {
+            const long long sr =
+                clampi(iy - cy_of(d), 0, ny - 1) + (long long)ny * clampi(iz - cz_of(d), 0, nz - 1);
+            bulk_load(dst + (size_t)d * pitch, fs + d * plane + sr * pitch, row_bytes, &full[s]);
+          }
+          bulk_load(scls + ((size_t)s * RY + yy) * pitch, a.cls + r * pitch, (uint32_t)pitch, &full[s]);
+        }
+        issued = j + 1;
+      }
+      if (failed) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
+      // No copy may still be in flight when the CTA exits: wait (bounded) for the
+      // last phase issued into every slot; completed phases return at once.
+      for (int s = 0; s < S_ && s < issued; ++s) {
+        const int last = s + ((issued - 1 - s) / S_) * S_;
+        mbar_wait(&full[s], (uint32_t)((last / S_) & 1), kWaitLimit);
+      }
+    }
+  } else {
+    // ---------------- consumer warps ----------------
+    const int pslot = (a.step_index + 1) & 1;  // pending rescale of the previous step
+    const int apply = a.st->apply[pslot];
+    const double corr = apply ? a.st->corr[pslot] : 1.0;
+    const float corrf = (float)corr;
+    const float corrf_s = corrf * F16S_INV_SCALE;
+    const int ry = warp / wpr;                    // row of the item this warp works on
+    const int xslot0 = (warp % wpr) * 32 + lane;  // slot of this thread in the first chunk
+    const int nchunks = (nx + shift + span - 1) / span;
+    int my_nan = 0;
+
+    for (int j = 0; j < my_count; ++j) {
+      const int s = j % S_;
+      if (!mbar_wait(&full[s], (uint32_t)((j / S_) & 1), kWaitLimit)) {
+        failed = true;
+        break;
+      }
+      const long long row = (blockIdx.x + (long long)j * gridDim.x) * RY + ry;
+      const bool row_ok = row < rows;
+      const int iy = row_ok ? (int)(row % ny) : 0;
+      const int iz = row_ok ? (int)(row / ny) : 0;
+      const T* sp = spop + ((size_t)s * RY + ry) * 19 * pitch;
+      const uint8_t* sc = scls + ((size_t)s * RY + ry) * pitch;
+      const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
+      const long long dense_row = row * nx;
+      const long long pop_row = row * pitch;
+
+      for (int c = 0; c < nchunks; ++c) {
+        const int ix = xslot0 + c * span - shift;
+        const bool active = row_ok && ix >= 0 && ix < nx;
+        const int lx = (ix >= 0 && ix < nx) ? ix : 1;  // lanes outside the row read cell 1
+        const uint8_t cl = sc[lx];
+        const int flag = cl & CLS_FLAG_MASK;
+        const bool solid = !active || flag == CELL_SOLID;
+        const bool xface = (ix == 0 || ix == nx - 1);
+        Real v[19];
+        Mac mr, mx, my, mz;
+
+        // ---- pull-stream (lbmCpuReference.ts:189-231) from the staged rows.  Every
+        // lane loads and collides; for cells outside the fluid interior (x faces,
+        // solids, lanes past the row) the values read at x - c_x stay inside the slot
+        // and the results are discarded or overwritten below. ----
+#pragma unroll
+        for (int d = 0; d < 19; ++d) {
+          const T raw = sp[d * pitch + lx - cx_of(d)];
+          if constexpr (MODE == MODE_FAST) v[d] = S::h_scaled(raw, d, corrf, corrf_s);
+          else if constexpr (MODE == MODE_MIRROR) v[d] = (double)(float)(S::f_of(raw, d) * corr);
+          else v[d] = S::f_of(raw, d) * corr;
+        }
+        if (c == nchunks - 1) {  // every value of this slot is in registers: release it
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&empty[s]);
+        }
+        const bool near = !solid && !xface && (cl & CLS_NEAR);
+        if (__any_sync(0xffffffffu, near)) {
+          if (near) {
+            // Bouzidi interpolated bounce-back for solid pull sources (:196-221).
+            const int bi = (flag == CELL_BOUNDARY) ? a.bmap[dense_row + ix] : -1;
+            auto popf = [&](int dd, long long prow, int px) -> double {
+              const double f = S::f_of(fs[dd * plane + prow * pitch + px], dd);
               if constexpr (MODE == MODE_MIRROR) return (double)(float)(f * corr);
               else return f * corr;
             };
-            const double fo = popf(wd, idx);
-            const int fxi = clampi(ix + cx_of(d), 0, nx - 1);
-            const int fyi = clampi(iy + cy_of(d), 0, ny - 1);
-            const int fzi = clampi(iz + cz_of(d), 0, nz - 1);
-            const long long ff = fxi + (long long)nx * (fyi + (long long)ny * fzi);
-            double val;
-            if ((a.cls[ff] & CLS_FLAG_MASK) != CELL_SOLID) {
-              if (qe < 0.5) {
-                const double fon = popf(wd, ff);
-                val = 2.0 * qe * fo + (1.0 - 2.0 * qe) * fon;
-              } else {
-                const double fic = popf(d, idx);
-                const double inv2q = 1.0 / (2.0 * qe);
-                val = inv2q * fo + (1.0 - inv2q) * fic;
+#pragma unroll 1
+            for (int d = 1; d < 19; ++d) {
+              const long long sr =
+                  clampi(iy - cy_rt(d), 0, ny - 1) + (long long)ny * clampi(iz - cz_rt(d), 0, nz - 1);
+              if ((a.cls[sr * pitch + ix - cx_rt(d)] & CLS_FLAG_MASK) == CELL_SOLID) {
+                const int wd = opp_of(d);
+                const double qv = bi >= 0 ? (double)a.q[(long long)bi * 18 + (wd - 1)] : 0.5;
+                const double qe = qv > 0.0 ? qv : 0.5;
+                const double fo = popf(wd, row, ix);
+                const int fxi = clampi(ix + cx_rt(d), 0, nx - 1);
+                const long long frow =
+                    clampi(iy + cy_rt(d), 0, ny - 1) + (long long)ny * clampi(iz + cz_rt(d), 0, nz - 1);
+                double val;
+                if ((a.cls[frow * pitch + fxi] & CLS_FLAG_MASK) != CELL_SOLID) {
+                  if (qe < 0.5) {
+                    const double fon = popf(wd, frow, fxi);
+                    val = 2.0 * qe * fo + (1.0 - 2.0 * qe) * fon;
+                  } else {
+                    const double fic = popf(d, row, ix);
+                    const double inv2q = 1.0 / (2.0 * qe);
+                    val = inv2q * fo + (1.0 - inv2q) * fic;
+                  }
+                } else {
+                  val = fo;
+                }
+                set_rt(v, d, MODE == MODE_FAST ? (Real)(val - w32_of_rt(d)) : (Real)val);
               }
-            } else {
-              val = fo;
             }
-            if constexpr (MODE == MODE_FAST) v[d] = (float)(val - (double)wf_of(d));
-            else v[d] = val;
           }
         }
-      }
-      // ---- collision (:233-304) ----
-      Real r, ux, uy, uz;
-      if constexpr (MODE == MODE_FAST) collide_f32(v, r, ux, uy, uz, (float)a.tau0, (float)a.k_smag);
-      else collide_f64<MODE == MODE_MIRROR>(v, r, ux, uy, uz, a.tau0, a.k_smag);
-      mr = (Mac)r; mx = (Mac)ux; my = (Mac)uy; mz = (Mac)uz;
+        // ---- collision (:233-304) ----
+        {
+          Real r, ux, uy, uz;
+          if constexpr (MODE == MODE_FAST) collide_f32(v, r, ux, uy, uz, (float)a.tau0, (float)a.k_smag);
+          else collide_f64<MODE == MODE_MIRROR>(v, r, ux, uy, uz, a.tau0, a.k_smag);
+          mr = (Mac)r; mx = (Mac)ux; my = (Mac)uy; mz = (Mac)uz;
+        }
 
-      if (ix == 1) ex.rho1[ty] = (double)mr;
-      if (ix == nx - 2) {
+        // ---- inlet / outlet exchange inside the warp (:328-371) ----
+        const int cell_lo = c * span + (warp % wpr) * 32 - shift;  // cell of lane 0
+        const bool has_inlet = row_ok && cell_lo <= 0 && 0 <= cell_lo + 31;
+        const bool has_outlet = row_ok && cell_lo <= nx - 1 && nx - 1 <= cell_lo + 31;
+        if (has_inlet) {
+          const double rho1 = __shfl_sync(0xffffffffu, solid_at_one(ix, solid) ? 1.0 : (double)mr, 1 - cell_lo);
+          if (ix == 0 && !solid) {
+            // Velocity inlet with density relaxation (:328-352).
+            double uxi = a.u_inlet;
+            if (a.ground_no_slip) uxi = a.u_inlet * a.abl[iy];
+            double uyi = 0.0;
+            if (a.step_index < 120) uyi = 0.015 * a.u_inlet * a.sin_tab[(long long)a.step_index * ny + iy];
+            if constexpr (MODE == MODE_FAST) {
+              const float ri = 0.85f * (float)rho1 + 0.15f;
 #pragma unroll
-        for (int d = 0; d < 19; ++d) {
-          // value as the outlet will read it back from fDst
-          if constexpr (MODE == MODE_FAST) ex.fprev[ty][d] = (double)v[d];
-          else ex.fprev[ty][d] = S::f_of(S::raw_of_f(v[d], d), d);
+              for (int d = 0; d < 19; ++d) v[d] = heq32(d, ri, (float)uxi, (float)uyi, 0.f);
+              mr = (Mac)ri;
+            } else {
+              const double ri = 0.85 * rho1 + 0.15 * 1.0;
+#pragma unroll
+              for (int d = 0; d < 19; ++d) v[d] = feq64(d, ri, uxi, uyi, 0.0);
+              mr = (Mac)ri;
+            }
+            mx = (Mac)uxi; my = (Mac)uyi; mz = (Mac)0;
+          }
         }
-        ex.mprev[ty][0] = mr; ex.mprev[ty][1] = mx; ex.mprev[ty][2] = my; ex.mprev[ty][3] = mz;
-      }
-      // ---- wall conditions (:375-429), own-cell moments only ----
-      if (wall_row && flag == CELL_FLUID) {
-        if (iy == 0) {
-          if (a.ground_no_slip) { mx = (Mac)0; mz = (Mac)0; }
-          my = (Mac)0;
+        if (has_outlet) {
+          const int src = nx - 2 - cell_lo;
+          // The value the outlet reads from fDst: rounded through the storage type;
+          // a solid cell's populations are never written (:173-179), so it is read.
+          Real send[19];
+          const bool src_solid = (ix == nx - 2) && solid;
+#pragma unroll
+          for (int d = 0; d < 19; ++d) {
+            if (src_solid) {
+              const double f = S::f_of(fd[d * plane + pop_row + ix], d);
+              send[d] = MODE == MODE_FAST ? (Real)(f - (double)wf_of(d)) : (Real)f;
+            } else if constexpr (MODE == MODE_FAST) {
+              send[d] = v[d];
+            } else {
+              send[d] = S::f_of(S::raw_of_f(v[d], d), d);
+            }
+          }
+          const double m0 = __shfl_sync(0xffffffffu, src_solid ? 1.0 : (double)mr, src);
+          const double m1 = __shfl_sync(0xffffffffu, src_solid ? 0.0 : (double)mx, src);
+          const double m2 = __shfl_sync(0xffffffffu, src_solid ? 0.0 : (double)my, src);
+          const double m3 = __shfl_sync(0xffffffffu, src_solid ? 0.0 : (double)mz, src);
+#pragma unroll
+          for (int d = 0; d < 19; ++d) send[d] = __shfl_sync(0xffffffffu, send[d], src);
+          if (ix == nx - 1 && !solid) {
+            // Convective outlet (:354-371).
+            if constexpr (MODE == MODE_FAST) {
+              const float ro = (float)m0 * 0.85f + 0.15f;
+#pragma unroll
+              for (int d = 0; d < 19; ++d)
+                v[d] = 0.75f * send[d] + 0.25f * heq32(d, ro, (float)m1, (float)m2, (float)m3);
+              mr = (Mac)ro;
+            } else {
+              const double ro = m0 * 0.85 + 1.0 * 0.15;
+#pragma unroll
+              for (int d = 0; d < 19; ++d) v[d] = 0.75 * send[d] + 0.25 * feq64(d, ro, m1, m2, m3);
+              mr = (Mac)ro;
+            }
+            mx = (Mac)m1; my = (Mac)m2; mz = (Mac)m3;
+          }
         }
-        if (iy == ny - 1) my = (Mac)0;
-        if (nz > 4 && (iz == 0 || iz == nz - 1)) mz = (Mac)0;
+        if (wall_row) {
+          if (!solid && !xface && flag == CELL_FLUID) {
+            // ---- wall conditions (:375-429), own-cell moments only ----
+            if (iy == 0) {
+              if (a.ground_no_slip) { mx = (Mac)0; mz = (Mac)0; }
+              my = (Mac)0;
+            }
+            if (iy == ny - 1) my = (Mac)0;
+            if (nz > 4 && (iz == 0 || iz == nz - 1)) mz = (Mac)0;
 #pragma unroll
-        for (int d = 0; d < 19; ++d) {
-          if constexpr (MODE == MODE_FAST) v[d] = heq32(d, (float)mr, (float)mx, (float)my, (float)mz);
-          else v[d] = feq64(d, (double)mr, (double)mx, (double)my, (double)mz);
+            for (int d = 0; d < 19; ++d) {
+              if constexpr (MODE == MODE_FAST) v[d] = heq32(d, (float)mr, (float)mx, (float)my, (float)mz);
+              else v[d] = feq64(d, (double)mr, (double)mx, (double)my, (double)mz);
+            }
+          }
         }
-      }
-    } else if (active && solid) {
-      // Solid cells: macro (0, 0, 0, 1); populations are never written (:173-179).
-      if (ix == 1) ex.rho1[ty] = 1.0;
-      if (ix == nx - 2) {
+        if (!solid) {
+          T* out = fd + pop_row + ix;
 #pragma unroll
-        for (int d = 0; d < 19; ++d) ex.fprev[ty][d] = S::f_of(fd[d * stride + idx], d) - (DBL ? 0.0 : (double)wf_of(d));
-        ex.mprev[ty][0] = 1.0; ex.mprev[ty][1] = 0.0; ex.mprev[ty][2] = 0.0; ex.mprev[ty][3] = 0.0;
-      }
-    }
-    __syncthreads();
-    if (active && !solid && xface) {
-      if (ix == 0) {
-        // Velocity inlet with density relaxation (:328-352).
-        double uxi = a.u_inlet;
-        if (a.ground_no_slip) uxi = a.u_inlet * a.abl[iy];
-        double uyi = 0.0;
-        if (a.step_index < 120) uyi = 0.015 * a.u_inlet * a.sin_tab[(long long)a.step_index * ny + iy];
-        if constexpr (MODE == MODE_FAST) {
-          const float ri = 0.85f * (float)ex.rho1[ty] + 0.15f;
-#pragma unroll
-          for (int d = 0; d < 19; ++d) v[d] = heq32(d, ri, (float)uxi, (float)uyi, 0.f);
-          mr = (Mac)ri;
+          for (int d = 0; d < 19; ++d) {
+            if constexpr (MODE == MODE_FAST) out[d * plane] = S::raw_of_h(v[d], d);
+            else out[d * plane] = S::raw_of_f(v[d], d);
+          }
+          if (mr == mr) my_sum += rho_fixed(mr);
+          else my_nan = 1;
         } else {
-          const double ri = 0.85 * ex.rho1[ty] + 0.15 * 1.0;
-#pragma unroll
-          for (int d = 0; d < 19; ++d) v[d] = feq64(d, ri, uxi, uyi, 0.0);
-          mr = (Mac)ri;
+          mr = (Mac)1; mx = (Mac)0; my = (Mac)0; mz = (Mac)0;  // solid macro (:173-179)
         }
-        mx = (Mac)uxi; my = (Mac)uyi; mz = (Mac)0;
-      } else {
-        // Convective outlet (:354-371).
-        const double rp = ex.mprev[ty][0];
-        const double uxo = ex.mprev[ty][1], uyo = ex.mprev[ty][2], uzo = ex.mprev[ty][3];
-        if constexpr (MODE == MODE_FAST) {
-          const float ro = (float)rp * 0.85f + 0.15f;
-#pragma unroll
-          for (int d = 0; d < 19; ++d)
-            v[d] = 0.75f * (float)ex.fprev[ty][d] + 0.25f * heq32(d, ro, (float)uxo, (float)uyo, (float)uzo);
-          mr = (Mac)ro;
-        } else {
-          const double ro = rp * 0.85 + 1.0 * 0.15;
-#pragma unroll
-          for (int d = 0; d < 19; ++d)
-            v[d] = 0.75 * ex.fprev[ty][d] + 0.25 * feq64(d, ro, uxo, uyo, uzo);
-          mr = (Mac)ro;
+        if (active && a.write_macro) {
+          const long long di = dense_row + ix;
+          a.mux[di] = (float)mx; a.muy[di] = (float)my; a.muz[di] = (float)mz; a.mrho[di] = (float)mr;
         }
-        mx = (Mac)uxo; my = (Mac)uyo; mz = (Mac)uzo;
       }
     }
-    if (active && !solid) {
-#pragma unroll
-      for (int d = 0; d < 19; ++d) {
-        if constexpr (MODE == MODE_FAST) fd[d * stride + idx] = S::raw_of_h(v[d], d);
-        else fd[d * stride + idx] = S::raw_of_f(v[d], d);
-      }
-      if (mr == mr) my_sum += rho_fixed(mr);
-      else my_nan = 1;
-    }
-    if (active && a.write_macro) {
-      a.mux[idx] = (float)mx; a.muy[idx] = (float)my; a.muz[idx] = (float)mz; a.mrho[idx] = (float)mr;
-    }
-    __syncthreads();  // the exchange slots are reused by the next chunk
+    if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
+    if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
   }
 
   // ---- mean-density rescale (:431-455): CTA sum, last CTA finalises ----
-  const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
-  const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) my_sum += __shfl_down_sync(0xffffffffu, my_sum, o);
-  my_nan = __any_sync(0xffffffffu, my_nan);
   if (lane == 0) red[warp] = my_sum;
-  if (lane == 0 && my_nan) a.st->nan_seen = 1;
   __syncthreads();
   const int slot = a.step_index & 1;
-  if (warp == 0) {
-    long long s = lane < nwarps ? red[lane] : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-      atomicAdd(&a.st->rho_sum[slot], (unsigned long long)s);
-      __threadfence();
-      const unsigned int t = atomicAdd(&a.st->ticket[slot], 1u);
-      is_last = (t == gridDim.x - 1);
-    }
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int w = 0; w <= kConsumerWarps; ++w) s += red[w];
+    if (nan_flag) a.st->nan_seen = 1;
+    atomicAdd(&a.st->rho_sum[slot], (unsigned long long)s);
+    __threadfence();
+    const unsigned int t = atomicAdd(&a.st->ticket[slot], 1u);
+    is_last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (is_last && threadIdx.x == 0 && threadIdx.y == 0) {
+  if (is_last && threadIdx.x == 0) {
     __threadfence();
     const long long total = (long long)atomicAdd(&a.st->rho_sum[slot], 0ull);
     int ap = 0;
@@ -476,17 +687,18 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
   const int apply = a.prev_slot >= 0 ? a.st->apply[a.prev_slot] : 0;
   const double corr = apply ? a.st->corr[a.prev_slot] : 1.0;
   auto pop = [&](int d, long long i) -> double {
-    const double v = S::f_of(f[d * a.stride + i], d);
+    const double v = S::f_of(f[a.L.at(d, i)], d);
     if constexpr (MODE == MODE_MIRROR) return (double)(float)(v * corr);
     else return v * corr;
   };
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   if (b < a.B) {
     const long long ci = a.bcells[b];
-    const int ix = (int)(ci % a.nx);
-    const long long rem = (ci - ix) / a.nx;
-    const int iy = (int)(rem % a.ny);
-    const int iz = (int)((rem - iy) / a.ny);
+    const int nx = a.L.nx, ny = a.L.ny, nz = a.L.nz;
+    const int ix = (int)(ci % nx);
+    const long long rem = (ci - ix) / nx;
+    const int iy = (int)(rem % ny);
+    const int iz = (int)((rem - iy) / ny);
     double cfx = 0.0, cfy = 0.0, cfz = 0.0;
     double cut = 0.0;
 #pragma unroll
@@ -495,12 +707,12 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
       if (qv > 0.0) {
         const int od = opp_of(d);
         const double fo = pop(d, ci);
-        const int ax = clampi(ix + cx_of(od), 0, a.nx - 1);
-        const int ay = clampi(iy + cy_of(od), 0, a.ny - 1);
-        const int az = clampi(iz + cz_of(od), 0, a.nz - 1);
-        const long long ff = ax + (long long)a.nx * (ay + (long long)a.ny * az);
+        const int ax = clampi(ix + cx_of(od), 0, nx - 1);
+        const int ay = clampi(iy + cy_of(od), 0, ny - 1);
+        const int az = clampi(iz + cz_of(od), 0, nz - 1);
+        const long long ff = ax + (long long)nx * (ay + (long long)ny * az);
         double fi = fo;
-        if ((a.cls[ff] & CLS_FLAG_MASK) != 1) {
+        if ((a.cls[a.L.cls_at(ff)] & CLS_FLAG_MASK) != 1) {
           if (qv < 0.5) {
             const double fon = pop(d, ff);
             fi = 2.0 * qv * fo + (1.0 - 2.0 * qv) * fon;
@@ -517,9 +729,9 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
         if (d <= 6) cut += 1.0;
       }
     }
-    const double rx = (ix + 0.5) - 0.5 * a.nx;
-    const double ry = (iy + 0.5) - 0.5 * a.ny;
-    const double rz = (iz + 0.5) - 0.5 * a.nz;
+    const double rx = (ix + 0.5) - 0.5 * nx;
+    const double ry = (iy + 0.5) - 0.5 * ny;
+    const double rz = (iz + 0.5) - 0.5 * nz;
     acc[0] = cfx; acc[1] = cfy; acc[2] = cfz;
     acc[3] = ry * cfz - rz * cfy;
     acc[4] = rz * cfx - rx * cfz;

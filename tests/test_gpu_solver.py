@@ -206,3 +206,21 @@ def test_error_status_paths(gpu_engine_cls):
         eng.set_voxel_grid(bad, {})
     assert e.value.code == N.ERR_ARG
     assert eng.step_and_extract_slice(4) is None
+
+
+@pytest.mark.parametrize("dims", [(33, 12, 10), (97, 9, 7), (289, 6, 6), (3, 5, 6), (40, 20, 3), (64, 1, 8)])
+def test_mirror_bit_exact_awkward_lattices(gpu_engine_cls, oracle_mod, dims):
+    """Row lengths that shift the thread mapping (nx = 1 mod 32), split a row over
+    several chunks (nx > 256), the minimum nx = 3, thin domains and ny = 1."""
+    nx, ny, nz = dims
+    r = max(1.0, min(ny, nz) / 4.0)
+    c = meshes.lattice_center(nx, ny, nz, 1.0, (nx / 3, ny / 2 - 0.5, nz / 2 - 0.5))
+    mesh = meshes.icosphere(r, c, 2) if nx > 8 and ny > 2 else (np.zeros((0, 3), np.float32), None)
+    case = cases.Case("awkward", nx, ny, nz, mesh, 0.05, 0.01, 0.1, 60)
+    vox, orc, eng = _pair(gpu_engine_cls, oracle_mod, case, "f32_mirror")
+    orc.step(60, threads=1)
+    eng.step(60)
+    assert _bitdiff(eng.read_populations(), orc.f(0)) == 0
+    mg, mo = eng.read_macro(), orc.macro()
+    for k in ("ux", "uy", "uz", "rho"):
+        assert _bitdiff(mg[k], mo[k]) == 0, k
