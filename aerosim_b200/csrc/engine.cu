@@ -39,6 +39,9 @@ struct aerosim_engine {
   int occupancy = 0;
   int num_sms = 148;
   float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
+  int32_t* near_cells = nullptr;  // near-wall cells and their link table
+  NearLink* links = nullptr;
+  long long n_near = 0;
   double* abl = nullptr;
   double* sin_tab = nullptr;
   int tab_ny = 0;
@@ -127,7 +130,7 @@ int configure_step(aerosim_engine* h) {
     const size_t smem = step_smem_bytes(L, S, eb);
     if (smem > 227 * 1024) break;
     int occ = 0;
-    cudaError_t e = launch_step(h->cfg.precision, dummy, block, 0, smem, h->stream, &occ);
+    cudaError_t e = launch_step(h->cfg.precision, dummy, block, 0, smem, h->stream, &occ, nullptr);
     if (e != cudaSuccess || occ < 1) break;
     // keep deepening the ring while the residency does not drop
     if (best_s == 0 || (occ >= best_occ && S <= 4)) {
@@ -141,7 +144,7 @@ int configure_step(aerosim_engine* h) {
   h->smem = step_smem_bytes(L, best_s, eb);
   // the probes above raised the shared-memory attribute to their own sizes: set it
   // (and the occupancy) for the chosen configuration
-  CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ));
+  CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ, nullptr));
   h->occupancy = best_occ;
   const long long items = ((long long)L.ny * L.nz + rows_per_item(L.nx) - 1) / rows_per_item(L.nx);
   long long grid = (long long)best_occ * h->num_sms;
@@ -219,6 +222,84 @@ int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[
   CU(h, cudaMemsetAsync(ng.cls, CELL_SOLID, (size_t)ng.ny * ng.nz * nl.pitch, h->stream));
   CU(h, launch_classify(ng.flags, ng.cls, nl, h->stream));
   CU(h, cudaStreamSynchronize(h->stream));
+  {
+    // Near-wall cells (x faces excluded: the inlet and outlet overwrite them) and
+    // their link table: for each direction, how the reference's pull obtains the
+    // value (lbmCpuReference.ts:189-224), resolved once per voxel grid.
+    const long long N = ng.N;
+    std::vector<uint8_t> cls((size_t)ng.ny * ng.nz * nl.pitch);
+    std::vector<int32_t> bmap(N);
+    std::vector<float> q((size_t)std::max<long long>(ng.B, 1) * 18);
+    // (the table is rebuilt with every voxel grid; the layout nl decides the offsets)
+    CU(h, cudaMemcpy(cls.data(), ng.cls, cls.size(), cudaMemcpyDeviceToHost));
+    CU(h, cudaMemcpy(bmap.data(), ng.bmap, N * 4, cudaMemcpyDeviceToHost));
+    if (ng.B > 0) CU(h, cudaMemcpy(q.data(), ng.q, ng.B * 18 * 4, cudaMemcpyDeviceToHost));
+    auto flag_at = [&](int x, int y, int z) {
+      return cls[((size_t)y + (size_t)ng.ny * z) * nl.pitch + x] & CLS_FLAG_MASK;
+    };
+    auto clampi_h = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    std::vector<int32_t> nearv;
+    for (int iz = 0; iz < ng.nz; ++iz)
+      for (int iy = 0; iy < ng.ny; ++iy) {
+        const long long row = iy + (long long)ng.ny * iz;
+        for (int ix = 1; ix < ng.nx - 1; ++ix)
+          if (cls[row * nl.pitch + ix] & CLS_NEAR) nearv.push_back((int32_t)(row * ng.nx + ix));
+      }
+    const long long nn = (long long)nearv.size();
+    if ((long long)19 * nl.plane >= (1LL << 32))
+      return fail(h, AEROSIM_ERR_ARG, "lattice too large for 32-bit population offsets");
+    auto off = [&](int d, long long c) -> uint32_t {
+      const long long r = c / ng.nx;
+      return (uint32_t)((long long)d * nl.plane + r * nl.pitch + (c - r * ng.nx));
+    };
+    std::vector<NearLink> links(19 * std::max<long long>(nn, 1));
+    for (long long t = 0; t < nn; ++t) {
+      const long long cell = nearv[t];
+      const int ix = (int)(cell % ng.nx);
+      const long long row = cell / ng.nx;
+      const int iy = (int)(row % ng.ny), iz = (int)(row / ng.ny);
+      const int flag = flag_at(ix, iy, iz);
+      const int bi = flag == CELL_BOUNDARY ? bmap[cell] : -1;
+      for (int d = 0; d < 19; ++d) {
+        NearLink& L = links[(size_t)d * nn + t];
+        const int sx = clampi_h(ix - cx_of(d), 0, ng.nx - 1), sy = clampi_h(iy - cy_of(d), 0, ng.ny - 1),
+                  sz = clampi_h(iz - cz_of(d), 0, ng.nz - 1);
+        const long long src = sx + (long long)ng.nx * (sy + (long long)ng.ny * sz);
+        L.A = 1.0; L.B = 0.0;
+        if (d > 0 && flag_at(sx, sy, sz) == CELL_SOLID) {
+          // Bouzidi in the pull, lbmCpuReference.ts:196-221
+          const int wd = opp_of(d);
+          const double qv = bi >= 0 ? (double)q[(size_t)bi * 18 + (wd - 1)] : 0.5;
+          const double qe = qv > 0.0 ? qv : 0.5;
+          const int fx = clampi_h(ix + cx_of(d), 0, ng.nx - 1), fy = clampi_h(iy + cy_of(d), 0, ng.ny - 1),
+                    fz = clampi_h(iz + cz_of(d), 0, ng.nz - 1);
+          const long long ff = fx + (long long)ng.nx * (fy + (long long)ng.ny * fz);
+          L.o1 = off(wd, cell); L.d1 = wd;
+          L.o2 = L.o1; L.d2 = wd;
+          if (flag_at(fx, fy, fz) != CELL_SOLID) {
+            if (qe < 0.5) {
+              L.A = 2.0 * qe; L.B = 1.0 - 2.0 * qe;
+              L.o2 = off(wd, ff); L.d2 = wd;
+            } else {
+              const double inv2q = 1.0 / (2.0 * qe);
+              L.A = inv2q; L.B = 1.0 - inv2q;
+              L.o2 = off(d, cell); L.d2 = d;
+            }
+          }
+        } else {
+          L.o1 = off(d, src); L.d1 = d;
+          L.o2 = L.o1; L.d2 = d;
+        }
+      }
+    }
+    cudaFree(h->near_cells); cudaFree(h->links);
+    h->near_cells = nullptr; h->links = nullptr;
+    h->n_near = nn;
+    CU(h, cudaMalloc(&h->near_cells, std::max<long long>(nn, 1) * 4));
+    CU(h, cudaMalloc(&h->links, links.size() * sizeof(NearLink)));
+    if (nn) CU(h, cudaMemcpy(h->near_cells, nearv.data(), nn * 4, cudaMemcpyHostToDevice));
+    CU(h, cudaMemcpy(h->links, links.data(), links.size() * sizeof(NearLink), cudaMemcpyHostToDevice));
+  }
   if (h->f[0] && (nl.pitch != h->L.pitch || nl.plane != h->L.plane)) free_pops(h);
   free_grid(h->g);
   h->g = ng;
@@ -325,6 +406,7 @@ int aerosim_destroy(aerosim_engine* h) {
   free_grid(h->g);
   free_pops(h);
   cudaFree(h->abl); cudaFree(h->sin_tab); cudaFree(h->st);
+  cudaFree(h->near_cells); cudaFree(h->links);
   cudaFree(h->force_partials); cudaFree(h->force_ticket); cudaFree(h->force_out);
   cudaFree(h->stats_buf); cudaFree(h->staging);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -502,19 +584,24 @@ int aerosim_step(aerosim_engine* h, int32_t n) {
   a.mux = h->mux; a.muy = h->muy; a.muz = h->muz; a.mrho = h->mrho;
   a.abl = h->abl; a.sin_tab = h->sin_tab; a.st = h->st;
   a.L = h->L; a.fluid_count = h->fluid_count;
+  a.near_cells = h->near_cells; a.n_near = h->n_near;
+  a.links = h->links;
   a.stages = h->stages;
   a.ground_no_slip = h->cfg.ground_no_slip;
   a.u_inlet = h->cfg.u_inlet_lattice;
   a.tau0 = 3.0 * h->cfg.nu_lattice + 0.5;
   const double cs2 = h->cfg.smagorinsky_cs * h->cfg.smagorinsky_cs;
   a.k_smag = 18.0 * M_SQRT2 * cs2;
+  long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < n; ++s) {
     a.fsrc = h->f[h->cur];
     a.fdst = h->f[h->cur ^ 1];
     a.step_index = (int)h->step_index;
     a.write_macro = (s == n - 1) ? 1 : 0;
-    CU(h, launch_step(h->cfg.precision, a, h->block, h->grid, h->smem, h->stream, nullptr));
+    int nl = 0;
+    CU(h, launch_step(h->cfg.precision, a, h->block, h->grid, h->smem, h->stream, nullptr, &nl));
+    launches += nl;
     h->cur ^= 1;
     h->step_index += 1;
   }
@@ -525,7 +612,7 @@ int aerosim_step(aerosim_engine* h, int32_t n) {
   float ms = 0.f;
   CU(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->last_ms = ms;
-  h->last_launches = n;
+  h->last_launches = launches;
   if (dev_err) return fail(h, AEROSIM_ERR_DEVICE, "step: the shared-memory pipeline timed out (device error flag set)");
   return AEROSIM_OK;
 }

@@ -38,7 +38,7 @@ size_t precision_bytes(int precision);
 // occ != nullptr: only query the resident CTAs per SM (and raise the shared-memory
 // attribute) for this block and dynamic shared-memory size.
 cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s,
-                        int* occ);
+                        int* occ, int* launches);
 cudaError_t launch_forces(int precision, const ForceArgs& a, unsigned grid, cudaStream_t s);
 cudaError_t launch_classify(const uint8_t* flags, uint8_t* cls, const Layout& L, cudaStream_t s);
 cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, float* mux, float* muy,

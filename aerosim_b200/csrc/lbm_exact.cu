@@ -12,7 +12,7 @@
 namespace aerosim {
 
 cudaError_t launch_step_fast(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
-                             cudaStream_t s, int* occ);
+                             cudaStream_t s, int* occ, int* launches);
 
 size_t precision_bytes(int precision) {
   switch (precision) {
@@ -24,11 +24,11 @@ size_t precision_bytes(int precision) {
 }
 
 cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
-                        cudaStream_t s, int* occ) {
+                        cudaStream_t s, int* occ, int* launches) {
   switch (precision) {
-    case AEROSIM_PREC_F32_MIRROR: return step_entry<StoreF32, MODE_MIRROR>(a, block, grid, smem, s, occ);
-    case AEROSIM_PREC_F64: return step_entry<StoreF64, MODE_F64>(a, block, grid, smem, s, occ);
-    default: return launch_step_fast(precision, a, block, grid, smem, s, occ);
+    case AEROSIM_PREC_F32_MIRROR: return step_entry<StoreF32, MODE_MIRROR>(a, block, grid, smem, s, occ, launches);
+    case AEROSIM_PREC_F64: return step_entry<StoreF64, MODE_F64>(a, block, grid, smem, s, occ, launches);
+    default: return launch_step_fast(precision, a, block, grid, smem, s, occ, launches);
   }
 }
 

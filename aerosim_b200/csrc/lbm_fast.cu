@@ -10,11 +10,11 @@
 namespace aerosim {
 
 cudaError_t launch_step_fast(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
-                             cudaStream_t s, int* occ) {
+                             cudaStream_t s, int* occ, int* launches) {
   switch (precision) {
-    case AEROSIM_PREC_F32: return step_entry<StoreF32, MODE_FAST>(a, block, grid, smem, s, occ);
-    case AEROSIM_PREC_F16S: return step_entry<StoreF16S, MODE_FAST>(a, block, grid, smem, s, occ);
-    case AEROSIM_PREC_BF16S: return step_entry<StoreBF16S, MODE_FAST>(a, block, grid, smem, s, occ);
+    case AEROSIM_PREC_F32: return step_entry<StoreF32, MODE_FAST>(a, block, grid, smem, s, occ, launches);
+    case AEROSIM_PREC_F16S: return step_entry<StoreF16S, MODE_FAST>(a, block, grid, smem, s, occ, launches);
+    case AEROSIM_PREC_BF16S: return step_entry<StoreBF16S, MODE_FAST>(a, block, grid, smem, s, occ, launches);
     default: return cudaErrorInvalidValue;
   }
 }

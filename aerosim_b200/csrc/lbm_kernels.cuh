@@ -29,6 +29,8 @@ enum { MODE_FAST = 0, MODE_MIRROR = 1, MODE_F64 = 2 };
 #define AEROSIM_FAST_MIN_BLOCKS 2
 #endif
 
+struct NearLink;
+
 struct StepArgs {
   const void* fsrc;
   void* fdst;
@@ -44,6 +46,9 @@ struct StepArgs {
   StepState* st;
   Layout L;
   long long fluid_count;  // non-solid cells
+  const int32_t* near_cells;  // cells with a solid pull source, x faces excluded
+  long long n_near;
+  const NearLink* links;      // [19][n_near] link table of the near-wall cells
   int stages;             // depth of the shared-memory ring
   int step_index;
   int write_macro;
@@ -103,20 +108,7 @@ __device__ __forceinline__ float heq32(int d, float rho, float ux, float uy, flo
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// Runtime-direction lattice tables for loops that are deliberately not unrolled.
-__device__ __forceinline__ int cx_rt(int d) { return cx_of(d); }
-__device__ __forceinline__ int cy_rt(int d) { return cy_of(d); }
-__device__ __forceinline__ int cz_rt(int d) { return cz_of(d); }
-__device__ __forceinline__ double w32_of_rt(int d) { return w32_of(d); }
-// Writes v[d] for a runtime d without forcing the array into local memory.
-template <class R>
-__device__ __forceinline__ void set_rt(R (&v)[19], int d, R x) {
-#pragma unroll
-  for (int k = 0; k < 19; ++k)
-    if (k == d) v[k] = x;
-}
-// The inlet reads rho at ix = 1, which is 1 for a solid cell (:177).
-__device__ __forceinline__ bool solid_at_one(int ix, bool solid) { return ix == 1 && solid; }
+
 
 // ---------------------------------------------------------------------------
 // Collision kernels for one cell.  In: pulled values v[19] (already rescaled).
@@ -309,8 +301,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int li
   return false;
 }
 constexpr int kWaitLimit = 1 << 22;
-constexpr int kConsumerWarps = 8;
-constexpr int kStepThreads = (kConsumerWarps + 1) * 32;
+constexpr int kConsumerWarps = 8;                      // warps 0..7: x-rows
+constexpr int kProducerWarp = kConsumerWarps;          // warp 8: bulk copies
+constexpr int kHelperWarp = kConsumerWarps + 1;        // warp 9: near-wall cells
+constexpr int kStepThreads = (kConsumerWarps + 2) * 32;
 enum { STEP_ERR_PIPELINE_TIMEOUT = 1 };
 
 // Thread -> cell mapping of a row: cell ix = slot - shift with slot = lane + 32 * warp
@@ -333,31 +327,166 @@ __host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem)
 // before the first row or past the end of a row.
 constexpr size_t kSmemGuard = 64;
 __host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem) {
-  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 * (size_t)stages + 16;
+  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 * (size_t)stages + 16 +
+         2 * (size_t)L.ny * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
-// The fused step kernel.  Persistent CTAs of 8 consumer warps + 1 producer warp
-// walk the x-rows of the lattice.  The producer issues, per work item, 19 bulk
-// copies per destination row (the clamped source row of every direction plane)
-// plus the class-byte row into a ring of shared-memory slots; a slot's `full`
-// mbarrier completes when its bytes have landed.  Consumer warps own whole row
-// segments: they pull their 19 values from the slot (x-shift by indexing), release
-// the slot on its `empty` mbarrier, collide in registers, settle the inlet / outlet
-// with warp shuffles and store straight to the destination planes.  No CTA-wide
-// barrier is taken inside the row loop.
+// One launch per time step, main_kernel: a persistent CTA of 8 consumer warps, a
+// producer warp and a helper warp.  The producer streams x-rows into the shared
+// ring with bulk copies; the consumers walk the rows: pull, collide, wall
+// conditions (:375-429), inlet and outlet (:323-373), store.  Meanwhile the helper
+// warp takes the CTA's share of the near-wall cells (Bouzidi, :196-221; one lane
+// per cell from a link table built with the voxel grid).  A near-wall cell at
+// ix = 1 or nx-2 carries its row's inlet or outlet, which need its post-collision
+// values.  The last CTA takes the step's mean-density rescale decision (:431-455).
 // ---------------------------------------------------------------------------
+
+// Near-wall link table: the value pulled along direction d is  A * p1 + B * p2  with
+// p1, p2 populations at element offsets o1, o2 (rescaled like every load):
+//   plain        f_d(src)                          A = 1,       B = 0       src = clamp(x - c_d)
+//   q < 0.5      2q f_w(x) + (1 - 2q) f_w(ff)      A = 2q,      B = 1 - 2q  w = opp(d), ff = clamp(x + c_d)
+//   q >= 0.5     f_w(x) / 2q + (1 - 1/2q) f_d(x)   A = 1/2q,    B = 1 - 1/2q
+//   ff solid     f_w(x)                            A = 1,       B = 0
+// A and B are formed exactly as the reference forms them (lbmCpuReference.ts:211-220),
+// so A * p1 + B * p2 evaluates the same expression; with B = 0 it returns p1.
+struct NearLink {
+  uint32_t o1, o2;  // element offsets of p1, p2 (plane * direction + row * pitch + x)
+  uint32_t d1, d2;  // their directions (the shifted codecs decode with w_d)
+  double A, B;
+};
+
+// Shared-memory inlet tables appended after the ring: ux_in[ny], uy_in[ny].
+__host__ __device__ inline size_t step_inlet_bytes(const Layout& L) { return 2 * (size_t)L.ny * sizeof(double); }
+
+template <class S, int MODE>
+__device__ __forceinline__ void wall_feq(typename std::conditional<MODE == MODE_FAST, float, double>::type (&v)[19],
+                                         double r, double x, double y, double z) {
+#pragma unroll
+  for (int d = 0; d < 19; ++d) {
+    if constexpr (MODE == MODE_FAST) v[d] = heq32(d, (float)r, (float)x, (float)y, (float)z);
+    else v[d] = feq64(d, r, x, y, z);
+  }
+}
+
+// One near-wall cell: every pulled value from the link table (all loads issued up
+// front), collision, the deferred inlet / outlet of its row (ix = 1 or nx-2, from its
+// values before any wall condition), the wall condition when it applies, stores.
+// Returns the fixed-point density added to the step's sum; sets *nan on a NaN.
+template <class S, int MODE>
+__device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, double corr,
+                                               const double* s_uxi, const double* s_uyi, int* nan) {
+  using T = typename S::T;
+  using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
+  using Mac = typename MacroOf<T>::type;
+  const Layout L = a.L;
+  const int nx = L.nx, ny = L.ny, nz = L.nz, pitch = L.pitch;
+  const long long plane = L.plane;
+  const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
+  T* __restrict__ fd = static_cast<T*>(a.fdst);
+  long long add = 0;
+  const long long cell = a.near_cells[t];
+  const int ix = (int)(cell % nx);
+  const long long row = cell / nx;
+  const int iy = (int)(row % ny), iz = (int)(row / ny);
+  const long long pop_row = row * pitch;
+  const int flag = a.cls[pop_row + ix] & CLS_FLAG_MASK;
+  const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
+  auto resc = [&](double f) -> double {
+    if constexpr (MODE == MODE_MIRROR) return (double)(float)(f * corr);
+    else return f * corr;
+  };
+  Real v[19];
+#pragma unroll
+  for (int d = 0; d < 19; ++d) {
+    const NearLink lk = a.links[(long long)d * a.n_near + t];
+    const double p1 = S::f_of(fs[lk.o1], (int)lk.d1);
+    const double p2 = S::f_of(fs[lk.o2], (int)lk.d2);
+    const double val = lk.A * resc(p1) + lk.B * resc(p2);
+    if constexpr (MODE == MODE_FAST) v[d] = (float)(val - (double)wf_of(d));
+    else v[d] = val;
+  }
+  Mac mr, mx, my, mz;
+  {
+    Real r, ux, uy, uz;
+    if constexpr (MODE == MODE_FAST) collide_f32(v, r, ux, uy, uz, (float)a.tau0, (float)a.k_smag);
+    else collide_f64<MODE == MODE_MIRROR>(v, r, ux, uy, uz, a.tau0, a.k_smag);
+    mr = (Mac)r; mx = (Mac)ux; my = (Mac)uy; mz = (Mac)uz;
+  }
+  if (ix == 1 && (a.cls[pop_row] & CLS_FLAG_MASK) != CELL_SOLID) {
+    // deferred inlet (:328-352)
+    const long long ic = row * nx;
+    const double uxi = s_uxi[iy], uyi = s_uyi[iy];
+    const double ri = MODE == MODE_FAST ? (double)(0.85f * (float)mr + 0.15f) : 0.85 * (double)mr + 0.15 * 1.0;
+    T* out = fd + pop_row;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+      if constexpr (MODE == MODE_FAST) out[d * plane] = S::raw_of_h(heq32(d, (float)ri, (float)uxi, (float)uyi, 0.f), d);
+      else out[d * plane] = S::raw_of_f(feq64(d, ri, uxi, uyi, 0.0), d);
+    }
+    if (a.write_macro) {
+      a.mux[ic] = (float)uxi; a.muy[ic] = (float)uyi; a.muz[ic] = 0.0f; a.mrho[ic] = (float)(Mac)ri;
+    }
+    add += rho_fixed((Mac)ri);
+  }
+  if (ix == nx - 2 && (a.cls[pop_row + nx - 1] & CLS_FLAG_MASK) != CELL_SOLID) {
+    // deferred outlet (:354-371)
+    const long long oc = row * nx + nx - 1;
+    T* out = fd + pop_row + nx - 1;
+    Mac ro;
+    if constexpr (MODE == MODE_FAST) {
+      const float r2 = (float)mr * 0.85f + 0.15f;
+#pragma unroll
+      for (int d = 0; d < 19; ++d)
+        out[d * plane] = S::raw_of_h(0.75f * v[d] + 0.25f * heq32(d, r2, (float)mx, (float)my, (float)mz), d);
+      ro = (Mac)r2;
+    } else {
+      const double r2 = (double)mr * 0.85 + 1.0 * 0.15;
+#pragma unroll
+      for (int d = 0; d < 19; ++d) {
+        const double stored = S::f_of(S::raw_of_f(v[d], d), d);
+        out[d * plane] = S::raw_of_f(0.75 * stored + 0.25 * feq64(d, r2, (double)mx, (double)my, (double)mz), d);
+      }
+      ro = (Mac)r2;
+    }
+    if (a.write_macro) {
+      a.mux[oc] = (float)mx; a.muy[oc] = (float)my; a.muz[oc] = (float)mz; a.mrho[oc] = (float)ro;
+    }
+    add += rho_fixed(ro);
+  }
+  if (wall_row && flag == CELL_FLUID) {
+    if (iy == 0) {
+      if (a.ground_no_slip) { mx = (Mac)0; mz = (Mac)0; }
+      my = (Mac)0;
+    }
+    if (iy == ny - 1) my = (Mac)0;
+    if (nz > 4 && (iz == 0 || iz == nz - 1)) mz = (Mac)0;
+    wall_feq<S, MODE>(v, (double)mr, (double)mx, (double)my, (double)mz);
+  }
+  T* out = fd + pop_row + ix;
+#pragma unroll
+  for (int d = 0; d < 19; ++d) {
+    if constexpr (MODE == MODE_FAST) out[d * plane] = S::raw_of_h(v[d], d);
+    else out[d * plane] = S::raw_of_f(v[d], d);
+  }
+  if (a.write_macro) {
+    a.mux[cell] = (float)mx; a.muy[cell] = (float)my; a.muz[cell] = (float)mz; a.mrho[cell] = (float)mr;
+  }
+  if (mr == mr) add += rho_fixed(mr);
+  else *nan = 1;
+  return add;
+}
+
 template <class S, int MODE>
 __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST_MIN_BLOCKS : 1)
-    step_kernel(const StepArgs a) {
+    main_kernel(const StepArgs a) {
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
   using Mac = typename MacroOf<T>::type;
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ long long red[kConsumerWarps + 1];
+  __shared__ long long red[kConsumerWarps + 2];
   __shared__ int nan_flag;
-  __shared__ int is_last;
 
   const Layout L = a.L;
   const int nx = L.nx, ny = L.ny, nz = L.nz, pitch = L.pitch;
@@ -365,7 +494,7 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
   const int S_ = a.stages;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int shift = row_shift(nx), span = row_span(nx), RY = rows_per_item(nx);
-  const int wpr = span / 32;  // warps per row
+  const int wpr = span / 32;
   const long long rows = (long long)ny * nz;
   const long long n_items = (rows + RY - 1) / RY;
   const int my_count = blockIdx.x < n_items ? (int)((n_items - 1 - blockIdx.x) / gridDim.x + 1) : 0;
@@ -375,6 +504,8 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
   uint64_t* full = reinterpret_cast<uint64_t*>(
       (reinterpret_cast<uintptr_t>(scls + (size_t)S_ * RY * pitch + kSmemGuard) + 7) & ~uintptr_t(7));
   uint64_t* empty = full + S_;
+  double* s_uxi = reinterpret_cast<double*>(empty + S_);
+  double* s_uyi = s_uxi + ny;
 
   const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
   T* __restrict__ fd = static_cast<T*>(a.fdst);
@@ -387,12 +518,29 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
     nan_flag = 0;
     mbar_fence_init();
   }
+  // inlet velocity per iy (:334-342), evaluated once per CTA
+  for (int i = threadIdx.x; i < ny; i += blockDim.x) {
+    double uxi = a.u_inlet;
+    if (a.ground_no_slip) uxi = a.u_inlet * a.abl[i];
+    double uyi = 0.0;
+    if (a.step_index < 120) uyi = 0.015 * a.u_inlet * a.sin_tab[(long long)a.step_index * ny + i];
+    s_uxi[i] = uxi;
+    s_uyi[i] = uyi;
+  }
   __syncthreads();
 
   long long my_sum = 0;
   bool failed = false;
 
-  if (warp == kConsumerWarps) {
+  if (warp == kHelperWarp) {
+    // ---------------- helper warp: this CTA's share of the near-wall cells ----------------
+    const int pslot = (a.step_index + 1) & 1;
+    const double corr = a.st->apply[pslot] ? a.st->corr[pslot] : 1.0;
+    int my_nan = 0;
+    for (long long t = (long long)blockIdx.x * 32 + lane; t < a.n_near; t += (long long)gridDim.x * 32)
+      my_sum += near_cell<S, MODE>(a, t, corr, s_uxi, s_uyi, &my_nan);
+    if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
+  } else if (warp == kProducerWarp) {
     // ---------------- producer warp ----------------
     if (lane == 0) {
       const uint32_t row_bytes = (uint32_t)(pitch * sizeof(T));
@@ -435,8 +583,7 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
     const double corr = apply ? a.st->corr[pslot] : 1.0;
     const float corrf = (float)corr;
     const float corrf_s = corrf * F16S_INV_SCALE;
-    const int ry = warp / wpr;                    // row of the item this warp works on
-    const int xslot0 = (warp % wpr) * 32 + lane;  // slot of this thread in the first chunk
+    const int ry = warp / wpr;
     const int nchunks = (nx + shift + span - 1) / span;
     int my_nan = 0;
 
@@ -446,6 +593,10 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
         failed = true;
         break;
       }
+      // The row-end warps carry the inlet and outlet: rotate the segment each warp
+      // takes from item to item so that extra work is spread over all warps.
+      const int seg = (warp % wpr + j) % wpr;
+      const int xslot0 = seg * 32 + lane;
       const long long row = (blockIdx.x + (long long)j * gridDim.x) * RY + ry;
       const bool row_ok = row < rows;
       const int iy = row_ok ? (int)(row % ny) : 0;
@@ -464,13 +615,11 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
         const int flag = cl & CLS_FLAG_MASK;
         const bool solid = !active || flag == CELL_SOLID;
         const bool xface = (ix == 0 || ix == nx - 1);
+        const bool near = (cl & CLS_NEAR) != 0;
         Real v[19];
-        Mac mr, mx, my, mz;
-
         // ---- pull-stream (lbmCpuReference.ts:189-231) from the staged rows.  Every
-        // lane loads and collides; for cells outside the fluid interior (x faces,
-        // solids, lanes past the row) the values read at x - c_x stay inside the slot
-        // and the results are discarded or overwritten below. ----
+        // lane loads and collides; x faces, near-wall cells and solids overwrite or
+        // discard the result. ----
 #pragma unroll
         for (int d = 0; d < 19; ++d) {
           const T raw = sp[d * pitch + lx - cx_of(d)];
@@ -482,66 +631,24 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
         }
-        const bool near = !solid && !xface && (cl & CLS_NEAR);
-        if (__any_sync(0xffffffffu, near)) {
-          if (near) {
-            // Bouzidi interpolated bounce-back for solid pull sources (:196-221).
-            const int bi = (flag == CELL_BOUNDARY) ? a.bmap[dense_row + ix] : -1;
-            auto popf = [&](int dd, long long prow, int px) -> double {
-              const double f = S::f_of(fs[dd * plane + prow * pitch + px], dd);
-              if constexpr (MODE == MODE_MIRROR) return (double)(float)(f * corr);
-              else return f * corr;
-            };
-#pragma unroll 1
-            for (int d = 1; d < 19; ++d) {
-              const long long sr =
-                  clampi(iy - cy_rt(d), 0, ny - 1) + (long long)ny * clampi(iz - cz_rt(d), 0, nz - 1);
-              if ((a.cls[sr * pitch + ix - cx_rt(d)] & CLS_FLAG_MASK) == CELL_SOLID) {
-                const int wd = opp_of(d);
-                const double qv = bi >= 0 ? (double)a.q[(long long)bi * 18 + (wd - 1)] : 0.5;
-                const double qe = qv > 0.0 ? qv : 0.5;
-                const double fo = popf(wd, row, ix);
-                const int fxi = clampi(ix + cx_rt(d), 0, nx - 1);
-                const long long frow =
-                    clampi(iy + cy_rt(d), 0, ny - 1) + (long long)ny * clampi(iz + cz_rt(d), 0, nz - 1);
-                double val;
-                if ((a.cls[frow * pitch + fxi] & CLS_FLAG_MASK) != CELL_SOLID) {
-                  if (qe < 0.5) {
-                    const double fon = popf(wd, frow, fxi);
-                    val = 2.0 * qe * fo + (1.0 - 2.0 * qe) * fon;
-                  } else {
-                    const double fic = popf(d, row, ix);
-                    const double inv2q = 1.0 / (2.0 * qe);
-                    val = inv2q * fo + (1.0 - inv2q) * fic;
-                  }
-                } else {
-                  val = fo;
-                }
-                set_rt(v, d, MODE == MODE_FAST ? (Real)(val - w32_of_rt(d)) : (Real)val);
-              }
-            }
-          }
-        }
-        // ---- collision (:233-304) ----
+        Mac mr, mx, my, mz;
         {
           Real r, ux, uy, uz;
           if constexpr (MODE == MODE_FAST) collide_f32(v, r, ux, uy, uz, (float)a.tau0, (float)a.k_smag);
           else collide_f64<MODE == MODE_MIRROR>(v, r, ux, uy, uz, a.tau0, a.k_smag);
           mr = (Mac)r; mx = (Mac)ux; my = (Mac)uy; mz = (Mac)uz;
         }
+        bool done = active && !solid && !xface && !near;  // this lane stores its cell
 
-        // ---- inlet / outlet exchange inside the warp (:328-371) ----
-        const int cell_lo = c * span + (warp % wpr) * 32 - shift;  // cell of lane 0
-        const bool has_inlet = row_ok && cell_lo <= 0 && 0 <= cell_lo + 31;
-        const bool has_outlet = row_ok && cell_lo <= nx - 1 && nx - 1 <= cell_lo + 31;
-        if (has_inlet) {
-          const double rho1 = __shfl_sync(0xffffffffu, solid_at_one(ix, solid) ? 1.0 : (double)mr, 1 - cell_lo);
-          if (ix == 0 && !solid) {
-            // Velocity inlet with density relaxation (:328-352).
-            double uxi = a.u_inlet;
-            if (a.ground_no_slip) uxi = a.u_inlet * a.abl[iy];
-            double uyi = 0.0;
-            if (a.step_index < 120) uyi = 0.015 * a.u_inlet * a.sin_tab[(long long)a.step_index * ny + iy];
+        // ---- inlet / outlet (:323-373), inside the warp that holds the row end ----
+        const int cell_lo = c * span + seg * 32 - shift;  // cell of lane 0
+        if (row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
+          const int src = 1 - cell_lo;
+          // rho at ix = 1 is 1 for a solid (:177); a near-wall ix = 1 defers the inlet
+          const double rho1 = __shfl_sync(0xffffffffu, solid ? 1.0 : (double)mr, src);
+          const int defer = __shfl_sync(0xffffffffu, (int)(near && !solid), src);
+          if (ix == 0 && !solid && !defer) {
+            const double uxi = s_uxi[iy], uyi = s_uyi[iy];
             if constexpr (MODE == MODE_FAST) {
               const float ri = 0.85f * (float)rho1 + 0.15f;
 #pragma unroll
@@ -554,65 +661,65 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
               mr = (Mac)ri;
             }
             mx = (Mac)uxi; my = (Mac)uyi; mz = (Mac)0;
+            done = true;
           }
         }
-        if (has_outlet) {
+        if (row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31) {
           const int src = nx - 2 - cell_lo;
-          // The value the outlet reads from fDst: rounded through the storage type;
-          // a solid cell's populations are never written (:173-179), so it is read.
-          Real send[19];
-          const bool src_solid = (ix == nx - 2) && solid;
+          const int defer = __shfl_sync(0xffffffffu, (int)(near && !solid), src);
+          if (!defer) {
+            // the outlet reads fDst at nx-2 before the walls (:363): the stored value,
+            // or for a solid cell whatever fDst holds there (never written)
+            Real send[19];
+            const bool stale = (ix == nx - 2) && solid;
 #pragma unroll
-          for (int d = 0; d < 19; ++d) {
-            if (src_solid) {
-              const double f = S::f_of(fd[d * plane + pop_row + ix], d);
-              send[d] = MODE == MODE_FAST ? (Real)(f - (double)wf_of(d)) : (Real)f;
-            } else if constexpr (MODE == MODE_FAST) {
-              send[d] = v[d];
-            } else {
-              send[d] = S::f_of(S::raw_of_f(v[d], d), d);
+            for (int d = 0; d < 19; ++d) {
+              if (stale) {
+                const double f = S::f_of(fd[d * plane + pop_row + ix], d);
+                send[d] = MODE == MODE_FAST ? (Real)(f - (double)wf_of(d)) : (Real)f;
+              } else if constexpr (MODE == MODE_FAST) {
+                send[d] = v[d];
+              } else {
+                send[d] = S::f_of(S::raw_of_f(v[d], d), d);
+              }
             }
-          }
-          const double m0 = __shfl_sync(0xffffffffu, src_solid ? 1.0 : (double)mr, src);
-          const double m1 = __shfl_sync(0xffffffffu, src_solid ? 0.0 : (double)mx, src);
-          const double m2 = __shfl_sync(0xffffffffu, src_solid ? 0.0 : (double)my, src);
-          const double m3 = __shfl_sync(0xffffffffu, src_solid ? 0.0 : (double)mz, src);
+            const double m0 = __shfl_sync(0xffffffffu, stale ? 1.0 : (double)mr, src);
+            const double m1 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)mx, src);
+            const double m2 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)my, src);
+            const double m3 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)mz, src);
 #pragma unroll
-          for (int d = 0; d < 19; ++d) send[d] = __shfl_sync(0xffffffffu, send[d], src);
-          if (ix == nx - 1 && !solid) {
-            // Convective outlet (:354-371).
-            if constexpr (MODE == MODE_FAST) {
-              const float ro = (float)m0 * 0.85f + 0.15f;
+            for (int d = 0; d < 19; ++d) send[d] = __shfl_sync(0xffffffffu, send[d], src);
+            if (ix == nx - 1 && !solid) {
+              if constexpr (MODE == MODE_FAST) {
+                const float ro = (float)m0 * 0.85f + 0.15f;
 #pragma unroll
-              for (int d = 0; d < 19; ++d)
-                v[d] = 0.75f * send[d] + 0.25f * heq32(d, ro, (float)m1, (float)m2, (float)m3);
-              mr = (Mac)ro;
-            } else {
-              const double ro = m0 * 0.85 + 1.0 * 0.15;
+                for (int d = 0; d < 19; ++d)
+                  v[d] = 0.75f * send[d] + 0.25f * heq32(d, ro, (float)m1, (float)m2, (float)m3);
+                mr = (Mac)ro;
+              } else {
+                const double ro = m0 * 0.85 + 1.0 * 0.15;
 #pragma unroll
-              for (int d = 0; d < 19; ++d) v[d] = 0.75 * send[d] + 0.25 * feq64(d, ro, m1, m2, m3);
-              mr = (Mac)ro;
+                for (int d = 0; d < 19; ++d) v[d] = 0.75 * send[d] + 0.25 * feq64(d, ro, m1, m2, m3);
+                mr = (Mac)ro;
+              }
+              mx = (Mac)m1; my = (Mac)m2; mz = (Mac)m3;
+              done = true;
             }
-            mx = (Mac)m1; my = (Mac)m2; mz = (Mac)m3;
           }
         }
+        // ---- wall conditions (:375-429): own moments, floor, ceiling, then sides ----
         if (wall_row) {
-          if (!solid && !xface && flag == CELL_FLUID) {
-            // ---- wall conditions (:375-429), own-cell moments only ----
+          if (done && !xface && flag == CELL_FLUID) {
             if (iy == 0) {
               if (a.ground_no_slip) { mx = (Mac)0; mz = (Mac)0; }
               my = (Mac)0;
             }
             if (iy == ny - 1) my = (Mac)0;
             if (nz > 4 && (iz == 0 || iz == nz - 1)) mz = (Mac)0;
-#pragma unroll
-            for (int d = 0; d < 19; ++d) {
-              if constexpr (MODE == MODE_FAST) v[d] = heq32(d, (float)mr, (float)mx, (float)my, (float)mz);
-              else v[d] = feq64(d, (double)mr, (double)mx, (double)my, (double)mz);
-            }
+            wall_feq<S, MODE>(v, (double)mr, (double)mx, (double)my, (double)mz);
           }
         }
-        if (!solid) {
+        if (done) {
           T* out = fd + pop_row + ix;
 #pragma unroll
           for (int d = 0; d < 19; ++d) {
@@ -621,12 +728,14 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
           }
           if (mr == mr) my_sum += rho_fixed(mr);
           else my_nan = 1;
-        } else {
-          mr = (Mac)1; mx = (Mac)0; my = (Mac)0; mz = (Mac)0;  // solid macro (:173-179)
         }
-        if (active && a.write_macro) {
+        if (a.write_macro) {
           const long long di = dense_row + ix;
-          a.mux[di] = (float)mx; a.muy[di] = (float)my; a.muz[di] = (float)mz; a.mrho[di] = (float)mr;
+          if (active && solid) {  // solid macro (:173-179)
+            a.mux[di] = 0.0f; a.muy[di] = 0.0f; a.muz[di] = 0.0f; a.mrho[di] = 1.0f;
+          } else if (done) {
+            a.mux[di] = (float)mx; a.muy[di] = (float)my; a.muz[di] = (float)mz; a.mrho[di] = (float)mr;
+          }
         }
       }
     }
@@ -634,22 +743,23 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
     if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
   }
 
-  // ---- mean-density rescale (:431-455): CTA sum, last CTA finalises ----
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) my_sum += __shfl_down_sync(0xffffffffu, my_sum, o);
   if (lane == 0) red[warp] = my_sum;
   __syncthreads();
   const int slot = a.step_index & 1;
+  __shared__ int is_last;
   if (threadIdx.x == 0) {
     long long s = 0;
-    for (int w = 0; w <= kConsumerWarps; ++w) s += red[w];
+    for (int w = 0; w < kConsumerWarps + 2; ++w) s += red[w];
     if (nan_flag) a.st->nan_seen = 1;
-    atomicAdd(&a.st->rho_sum[slot], (unsigned long long)s);
+    if (s) atomicAdd(&a.st->rho_sum[slot], (unsigned long long)s);
     __threadfence();
-    const unsigned int t = atomicAdd(&a.st->ticket[slot], 1u);
-    is_last = (t == gridDim.x - 1);
+    const unsigned int tk = atomicAdd(&a.st->ticket[slot], 1u);
+    is_last = (tk == gridDim.x - 1);
   }
   __syncthreads();
+  // ---- mean-density rescale (:431-455): the last CTA takes the decision ----
   if (is_last && threadIdx.x == 0) {
     __threadfence();
     const long long total = (long long)atomicAdd(&a.st->rho_sum[slot], 0ull);

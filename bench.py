@@ -1,0 +1,334 @@
+"""Benchmark of the B200 solver hot path: D3Q19 stream/collide MLUPS at 256x128x128.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one lattice time step of the whole lattice): the seeded
+perturbed-ellipsoid case on a 256 x 128 x 128 D3Q19 lattice (20480-triangle mesh,
+u = 0.08, Re = 2e4 on the body length, Cs = 0.1), FP32 populations.  Synthetic
+input: the mesh is generated from a fixed seed; no dataset is read.
+
+Prints one JSON line (rank 0).  `value` is whole-job MLUPS measured with CUDA events
+around exactly K steps (inputs resident in HBM; the populations, 637 MB, exceed the
+126 MB L2, so no flush is needed).  `e2e` is the same metric through the C-ABI frame
+loop of the reference's solver interface: aerosim_step(4 substeps) followed by the
+force readout to the host, timed on the host clock.  Under torchrun every rank runs
+its own lattice (independent shards, weak scaling); times are the max over ranks.
+
+--impl reference times the reference algorithm's CPU implementation on the host
+cores: the reference is TypeScript and no JavaScript runtime exists on this machine,
+so it is the C++ restatement in oracle/ (the correctness oracle), OpenMP over all
+host threads, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS and HBM-roofline % at 256x128x128, FP32 vs FP16-store; Cd err vs FP64"
+WORKLOAD = "ellipsoid_256x128x128"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic(precision: str):
+    """DRAM bytes per step-kernel launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "main_kernel_ellipsoid_256x128x128.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(rf"dram_bytes_per_launch_{precision}:\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _make_engine(case, precision: str, device: int):
+    from aerosim_b200 import LBMEngine, frontal_area
+    eng = LBMEngine(device)
+    pos = case.mesh[0]
+    cfg = {"uInletLattice": case.u_inlet, "nuLattice": case.nu, "smagorinskyCs": case.cs,
+           "precision": precision, "frontalAreaM2": frontal_area(case.mesh),
+           "characteristicLengthM": float(pos[:, 0].max() - pos[:, 0].min())}
+    info = eng.voxelize(case.mesh, None, case.tunnel, {"nx": case.nx, "ny": case.ny, "nz": case.nz}, cfg)
+    return eng, info
+
+
+def _timed_steps(eng, steps: int):
+    """CUDA-event time (ms) of exactly `steps` steps and the kernel launches they took."""
+    eng.step(steps)
+    return eng.last_step_timing()
+
+
+def run_ours(args) -> dict:
+    import torch
+    from aerosim_b200 import _native as N
+    from aerosim_b200 import cases
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = local
+    case = cases.ellipsoid_256x128x128(args.steps)
+    cells = case.cells
+
+    def barrier_sync():
+        torch.cuda.synchronize(dev)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    out = {}
+    # ---- headline: FP32, device-timed ----
+    eng, info = _make_engine(case, "f32", dev)
+    eng.step(args.warmup)
+    barrier_sync()
+    with ClockSampler(dev) as clk:
+        ms, launches = _timed_steps(eng, args.steps)
+    barrier_sync()
+    ms = max_over_ranks(ms)
+    mlups = ws * cells * args.steps / (ms * 1e-3) / 1e6
+    hbm, hbm_kind = _peaks()
+    bpc = N.BYTES_PER_CELL[N.PREC_F32]
+    achieved = cells * bpc / (ms / args.steps * 1e-3) / 1e9  # per-GPU GB/s of one step launch
+    traffic = _profile_traffic("f32")
+    out.update({
+        "value": round(mlups, 1), "ms_per_step": ms / args.steps, "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "peak_kind": hbm_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_cell": bpc,
+                     "note": f"algorithmic {bpc} B/cell x {cells} cells per launch / mean launch time"},
+        "voxelization_ms": info.voxelization_time_ms,
+        "boundary_cells": int(info.boundary_cell_count), "solid_cells": int(info.solid_cell_count),
+    })
+
+    # ---- e2e: frames of 4 substeps + force readout to the host through the C-ABI ----
+    frames = max(4, args.steps // 4)
+    for _ in range(2):
+        eng.step_and_extract_slice(4)
+    barrier_sync()
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        eng.step_and_extract_slice(4)
+    dt = time.perf_counter() - t0
+    barrier_sync()
+    dt = max_over_ranks(dt)
+    import ctypes
+    out["e2e"] = {"value": round(ws * cells * 4 * frames / dt / 1e6, 1), "unit": "MLUPS",
+                  "h2d_bytes_per_step": 0, "d2h_bytes_per_step": ctypes.sizeof(N.Forces) + 4,
+                  "frame": "aerosim_step(4 substeps) + aerosim_read_forces (FP64 sums, host copy)",
+                  "frames": frames}
+    eng.close()
+
+    # ---- FP16 / BF16 shifted storage: throughput ----
+    for prec in ("f16s", "bf16s"):
+        e2, _ = _make_engine(case, prec, dev)
+        e2.step(args.warmup)
+        barrier_sync()
+        ms2, _ = _timed_steps(e2, args.steps)
+        barrier_sync()
+        ms2 = max_over_ranks(ms2)
+        b2 = N.BYTES_PER_CELL[N.PRECISIONS[prec]]
+        ach2 = cells * b2 / (ms2 / args.steps * 1e-3) / 1e9
+        out[prec] = {"mlups": round(ws * cells * args.steps / (ms2 * 1e-3) / 1e6, 1),
+                     "ms_per_step": ms2 / args.steps, "speedup_vs_f32": round(ms / ms2, 3),
+                     "roofline": {"achieved": round(ach2, 1), "peak": hbm, "unit": "GB/s",
+                                  "frac": round(ach2 / hbm, 4), "traffic": _profile_traffic(prec)}}
+        e2.close()
+
+    # ---- Cd / Cl / Cm error of reduced storage vs the FP64 GPU run ----
+    if args.cd_steps > 0:
+        res = {}
+        for prec in ("f64", "f32", "f16s", "bf16s"):
+            e3, _ = _make_engine(case, prec, dev)
+            e3.step(args.cd_steps)
+            f = e3.read_forces()
+            m = e3.mass_stats()
+            res[prec] = {"cd": f.cd, "cl": f.cl, "cm": f.cm, "mass_drift": m["meanRho"] - 1.0,
+                         "cumulative_rescale": m["cumulativeRescale"]}
+            e3.close()
+        ref = res["f64"]
+        out["cd_err_vs_fp64"] = {"steps": args.cd_steps, "f64": ref, **{
+            p: {"dcd_rel": abs(res[p]["cd"] - ref["cd"]) / abs(ref["cd"]),
+                "dcl_abs": abs(res[p]["cl"] - ref["cl"]), "dcm_abs": abs(res[p]["cm"] - ref["cm"]),
+                "mass_drift": res[p]["mass_drift"]} for p in ("f32", "f16s", "bf16s")}}
+
+    # ---- CPU baseline: the oracle on one core, bounded sample ----
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_sample(case, threads=1, seconds=args.cpu_seconds)
+
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    out.update({
+        "metric": METRIC, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded perturbed-ellipsoid mesh generated in-process (no dataset)",
+        "config": {"workload": f"{WORKLOAD}_f32", "lattice": [case.nx, case.ny, case.nz], "cells_per_gpu": cells,
+                   "mesh_triangles": int(case.mesh[1].shape[0]), "u_inlet": case.u_inlet, "nu": case.nu,
+                   "smagorinsky_cs": case.cs, "storage": "f32", "collision": "f32",
+                   "l2": "inputs larger than L2 (637 MB of populations vs 126 MB L2), no flush",
+                   "parallelism": f"{ws} independent lattices, one per GPU (weak scaling)"},
+    })
+    return out if rank == 0 else {}
+
+
+def cpu_sample(case, threads: int, seconds: float, steps_cap: int | None = None) -> dict:
+    """Times the oracle (C++ restatement of the reference's CPU solver) on the same
+    workload: oracle voxelization, then whole-lattice steps until `seconds` pass."""
+    import oracle
+    vox = oracle.voxelize(case.mesh, None, float(case.ny), case.nx, case.ny, case.nz)
+    s = oracle.Solver(vox, u_inlet=case.u_inlet, nu=case.nu, cs=case.cs)
+    s.step(1, threads=threads)  # warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        s.step(1, threads=threads)
+        n += 1
+        if time.perf_counter() - t0 >= seconds or (steps_cap and n >= steps_cap):
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(case.cells * n / dt / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": f"{n} whole-lattice steps of {WORKLOAD} ({case.cells} cells) in {dt:.1f} s",
+            "host_threads_available": os.cpu_count()}
+
+
+def run_reference(args) -> dict:
+    from aerosim_b200 import cases
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return {}
+    import oracle
+    threads = oracle.max_threads()
+    case = cases.ellipsoid_256x128x128(args.steps)
+    # each "step" is one whole-lattice step; the timed count is capped so the run
+    # ends within a few minutes on the host cores
+    budget = float(os.environ.get("AEROSIM_REF_SECONDS", "120"))
+    vox = oracle.voxelize(case.mesh, None, float(case.ny), case.nx, case.ny, case.nz)
+    s = oracle.Solver(vox, u_inlet=case.u_inlet, nu=case.nu, cs=case.cs)
+    t0 = time.perf_counter()
+    s.step(max(1, min(args.warmup, 3)), threads=threads)
+    per = (time.perf_counter() - t0) / max(1, min(args.warmup, 3))
+    n = max(1, min(args.steps, int(budget / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    s.step(n, threads=threads)
+    dt = time.perf_counter() - t0
+    mlups = case.cells * n / dt / 1e6
+    return {"metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": ws, "steps": n,
+            "warmup": args.warmup, "ms_per_step": dt / n * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "impl": "reference",
+            "data": "synthetic: seeded perturbed-ellipsoid mesh generated in-process (no dataset)",
+            "config": {"workload": f"{WORKLOAD}_f32", "lattice": [case.nx, case.ny, case.nz],
+                       "cells_per_gpu": case.cells, "storage": "f32 (f64 arithmetic, like the reference)"},
+            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+                             "sample": f"{n} of the requested {args.steps} whole-lattice steps, "
+                                       f"OpenMP over {threads} threads (reference is TypeScript; "
+                                       "no JavaScript runtime here, so its C++ restatement runs)"},
+            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cd-steps", type=int, default=20000, help="steps of the FP64-oracle Cd comparison (0: skip)")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
