@@ -328,7 +328,7 @@ __host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem)
 constexpr size_t kSmemGuard = 64;
 __host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem) {
   return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 * (size_t)stages + 16 +
-         2 * (size_t)L.ny * sizeof(double);
+         2 * (size_t)L.ny * sizeof(double) + (size_t)stages * rows_per_item(L.nx) * sizeof(int2);
 }
 
 // ---------------------------------------------------------------------------
@@ -506,6 +506,7 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
   uint64_t* empty = full + S_;
   double* s_uxi = reinterpret_cast<double*>(empty + S_);
   double* s_uyi = s_uxi + ny;
+  int2* s_row = reinterpret_cast<int2*>(s_uyi + ny);  // [S_][RY] (iy, iz) of the slot's rows
 
   const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
   T* __restrict__ fd = static_cast<T*>(a.fdst);
@@ -553,10 +554,16 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
         }
         const long long r0 = (blockIdx.x + (long long)j * gridDim.x) * RY;
         const int nr = (int)(rows - r0 < RY ? rows - r0 : RY);
+        // row coordinates for the consumers, published by the arrive below
+        for (int yy = 0; yy < nr; ++yy) {
+          const int r = (int)(r0 + yy);
+          s_row[s * RY + yy] = make_int2(r % ny, r / ny);
+        }
         mbar_arrive_expect_tx(&full[s], (uint32_t)nr * (19u * row_bytes + (uint32_t)pitch));
         for (int yy = 0; yy < nr; ++yy) {
+          const int2 yz = s_row[s * RY + yy];
+          const int iy = yz.x, iz = yz.y;
           const long long r = r0 + yy;
-          const int iy = (int)(r % ny), iz = (int)(r / ny);
           T* dst = spop + ((size_t)s * RY + yy) * 19 * pitch;
 #pragma unroll
           for (int d = 0; d < 19; ++d) {
@@ -599,8 +606,12 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
       const int xslot0 = seg * 32 + lane;
       const long long row = (blockIdx.x + (long long)j * gridDim.x) * RY + ry;
       const bool row_ok = row < rows;
-      const int iy = row_ok ? (int)(row % ny) : 0;
-      const int iz = row_ok ? (int)(row / ny) : 0;
+      int iy = 0, iz = 0;
+      if (row_ok) {
+        const int2 yz = s_row[s * RY + ry];
+        iy = yz.x;
+        iz = yz.y;
+      }
       const T* sp = spop + ((size_t)s * RY + ry) * 19 * pitch;
       const uint8_t* sc = scls + ((size_t)s * RY + ry) * pitch;
       const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));

@@ -68,7 +68,7 @@ def _profile_traffic(precision: str):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples every 200 ms while the timed region runs."""
+    """nvidia-smi clock / throttle samples every 100 ms while the timed region runs."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -83,7 +83,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -222,22 +222,35 @@ def run_ours(args) -> dict:
                                   "frac": round(ach2 / hbm, 4), "traffic": _profile_traffic(prec)}}
         e2.close()
 
-    # ---- Cd / Cl / Cm error of reduced storage vs the FP64 GPU run ----
+    # ---- Cd / Cl / Cm error of reduced storage vs the FP64 GPU run.  The flow at
+    # Re = 2e4 is unsteady and chaotic, so runs that differ only in rounding drift
+    # apart sample by sample: the coefficients are compared as time averages over
+    # the second half of the run (a force sample every 100 steps). ----
     if args.cd_steps > 0:
         res = {}
+        half = args.cd_steps // 2
+        every = 100
         for prec in ("f64", "f32", "f16s", "bf16s"):
             e3, _ = _make_engine(case, prec, dev)
-            e3.step(args.cd_steps)
-            f = e3.read_forces()
+            e3.step(half)
+            cd, cl, cm = [], [], []
+            for _ in range(max(1, (args.cd_steps - half) // every)):
+                e3.step(every)
+                f = e3.read_forces()
+                cd.append(f.cd); cl.append(f.cl); cm.append(f.cm)
             m = e3.mass_stats()
-            res[prec] = {"cd": f.cd, "cl": f.cl, "cm": f.cm, "mass_drift": m["meanRho"] - 1.0,
-                         "cumulative_rescale": m["cumulativeRescale"]}
+            res[prec] = {"cd_mean": float(np.mean(cd)), "cl_mean": float(np.mean(cl)), "cm_mean": float(np.mean(cm)),
+                         "cd_std": float(np.std(cd)), "cd_last": cd[-1], "mass_drift": m["meanRho"] - 1.0,
+                         "cumulative_rescale": m["cumulativeRescale"], "nan": m["hasNaN"]}
             e3.close()
         ref = res["f64"]
-        out["cd_err_vs_fp64"] = {"steps": args.cd_steps, "f64": ref, **{
-            p: {"dcd_rel": abs(res[p]["cd"] - ref["cd"]) / abs(ref["cd"]),
-                "dcl_abs": abs(res[p]["cl"] - ref["cl"]), "dcm_abs": abs(res[p]["cm"] - ref["cm"]),
-                "mass_drift": res[p]["mass_drift"]} for p in ("f32", "f16s", "bf16s")}}
+        out["cd_err_vs_fp64"] = {"steps": args.cd_steps, "window": f"steps {half}..{args.cd_steps}, every {every}",
+                                 "f64": ref, **{
+            p: {"dcd_mean_rel": abs(res[p]["cd_mean"] - ref["cd_mean"]) / abs(ref["cd_mean"]),
+                "dcl_mean_abs": abs(res[p]["cl_mean"] - ref["cl_mean"]),
+                "dcm_mean_abs": abs(res[p]["cm_mean"] - ref["cm_mean"]),
+                "cd_mean": res[p]["cd_mean"], "cd_std": res[p]["cd_std"],
+                "mass_drift": res[p]["mass_drift"], "nan": res[p]["nan"]} for p in ("f32", "f16s", "bf16s")}}
 
     # ---- CPU baseline: the oracle on one core, bounded sample ----
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -316,7 +329,7 @@ def run_reference(args) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cd-steps", type=int, default=20000, help="steps of the FP64-oracle Cd comparison (0: skip)")
