@@ -97,6 +97,8 @@ SIGNATURES = {
     "aerosim_mass_stats": ([_P, C.POINTER(Mass)], C.c_int),
     "aerosim_last_step_timing": ([_P, _F64P, C.POINTER(C.c_int64)], C.c_int),
     "aerosim_frontal_area": ([_F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P], C.c_int),
+    "aerosim_momentum_exchange_noalloc": ([_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, C.c_int32, _P, _P],
+                                          C.c_int),
 }
 
 _lib = None

@@ -7,6 +7,7 @@ Translation units and their floating-point contracts:
   lbm_exact.cu  FP64 kernels mirroring the reference's rounding: -fmad=false
   voxelize.cu   FP64 BVH voxelizer, bit-exact flags and links: -fmad=false
   engine.cu     C-ABI host layer
+  noalloc.cu    allocation-free force reduction entry point: -fmad=false
 """
 from __future__ import annotations
 
@@ -32,6 +33,7 @@ UNITS = {
     "lbm_exact.cu": ["-fmad=false"],
     "voxelize.cu": ["-fmad=false"],
     "engine.cu": [],
+    "noalloc.cu": ["-fmad=false"],
 }
 
 

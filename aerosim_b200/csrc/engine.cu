@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -61,10 +62,15 @@ struct aerosim_engine {
 namespace {
 
 std::string g_create_error;
+std::mutex g_error_mu;
 
 int fail(aerosim_engine* h, int code, const std::string& msg) {
-  if (h) h->err = msg;
-  else g_create_error = msg;
+  if (h) {
+    h->err = msg;
+  } else {
+    std::lock_guard<std::mutex> lock(g_error_mu);
+    g_create_error = msg;
+  }
   return code;
 }
 
@@ -354,6 +360,10 @@ void coefficients(const aerosim_config& c, double dx, aerosim_forces* o) {
 }
 
 }  // namespace
+
+namespace aerosim {
+void set_global_error(const std::string& msg) { fail(nullptr, 0, msg); }
+}  // namespace aerosim
 
 extern "C" {
 

@@ -31,6 +31,9 @@ int run_voxelizer(const float* pos, int64_t nverts, const int32_t* idx, int64_t 
                   const double* world16, double tunnel_height, int nx, int ny, int nz,
                   cudaStream_t s, DevGrid* g, std::string* err);
 
+// Message returned by aerosim_last_error(NULL) (calls that take no engine handle).
+void set_global_error(const std::string& msg);
+
 // Element size of the population storage of a precision mode.
 size_t precision_bytes(int precision);
 

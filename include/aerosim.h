@@ -170,6 +170,25 @@ int aerosim_mass_stats(aerosim_engine* h, aerosim_mass* out);
  * engine's stream) and the number of kernels it launched. */
 int aerosim_last_step_timing(aerosim_engine* h, double* ms, int64_t* kernel_launches);
 
+/* ---- allocation-free force reduction ------------------------------------------ */
+
+/* Momentum-exchange forces (the reduction of aerosim_read_forces) over device buffers
+ * the caller owns, without allocating any device memory.  No counterpart in the
+ * reference: it serves hosts that own all device memory through their own allocator
+ * and may not call cudaMalloc, and frame loops that cannot afford its synchronisation.
+ * f: device float[19 * N], dense f[d * N + idx]; flags: device u8[N] (0 fluid, 1 solid,
+ * 2 boundary); boundary_cells: device i32[B]; q: device f32[B * 18]; out: device
+ * double[8] = fx, fy, fz, mx, my, mz (lattice units, moments about the domain centre),
+ * cut face links, CTAs used.  stream: a cudaStream_t (NULL: the legacy default stream);
+ * the work is enqueued, not waited for.  Limit: B <= 1 048 576 (4096 CTAs); larger B
+ * returns AEROSIM_ERR_ARG.  Scratch is a fixed per-device array shared by all calls:
+ * calls whose kernels overlap on the GPU race.  The first call on a device resolves the
+ * array's address and should come before any stream capture on that device.  Errors
+ * are reported through aerosim_last_error(NULL). */
+int aerosim_momentum_exchange_noalloc(const float* f, const uint8_t* flags, const int32_t* boundary_cells,
+                                      const float* q, int64_t boundary_count, int32_t nx, int32_t ny,
+                                      int32_t nz, double* out, void* stream);
+
 /* ---- host-side geometry inputs ------------------------------------------- */
 
 /* computeProjectedFrontalArea(geometry, worldMatrix, gridResolution),
