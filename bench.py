@@ -189,25 +189,26 @@ def run_ours(args) -> dict:
     })
 
     # ---- e2e: frames of 4 substeps + force readout to the host through the C-ABI ----
-    frames = max(4, args.steps // 4)
-    for _ in range(2):
-        eng.step_and_extract_slice(4)
-    barrier_sync()
-    t0 = time.perf_counter()
-    for _ in range(frames):
-        eng.step_and_extract_slice(4)
-    dt = time.perf_counter() - t0
-    barrier_sync()
-    dt = max_over_ranks(dt)
-    import ctypes
-    out["e2e"] = {"value": round(ws * cells * 4 * frames / dt / 1e6, 1), "unit": "MLUPS",
-                  "h2d_bytes_per_step": 0, "d2h_bytes_per_step": ctypes.sizeof(N.Forces) + 4,
-                  "frame": "aerosim_step(4 substeps) + aerosim_read_forces (FP64 sums, host copy)",
-                  "frames": frames}
+    frames = max(4, args.steps // 4) if not args.no_e2e else 0
+    if frames:
+        for _ in range(2):
+            eng.step_and_extract_slice(4)
+        barrier_sync()
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            eng.step_and_extract_slice(4)
+        dt = time.perf_counter() - t0
+        barrier_sync()
+        dt = max_over_ranks(dt)
+        import ctypes
+        out["e2e"] = {"value": round(ws * cells * 4 * frames / dt / 1e6, 1), "unit": "MLUPS",
+                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": ctypes.sizeof(N.Forces) + 4,
+                      "frame": "aerosim_step(4 substeps) + aerosim_read_forces (FP64 sums, host copy)",
+                      "frames": frames}
     eng.close()
 
     # ---- FP16 / BF16 shifted storage: throughput ----
-    for prec in ("f16s", "bf16s"):
+    for prec in [p for p in args.precisions.split(",") if p in ("f16s", "bf16s")]:
         e2, _ = _make_engine(case, prec, dev)
         e2.step(args.warmup)
         barrier_sync()
@@ -335,6 +336,9 @@ def main():
     ap.add_argument("--cd-steps", type=int, default=20000, help="steps of the FP64-oracle Cd comparison (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI frame loop")
+    ap.add_argument("--precisions", default="f32,f16s,bf16s",
+                    help="storage modes timed after the FP32 headline (f16s, bf16s)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
