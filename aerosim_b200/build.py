@@ -3,7 +3,8 @@
 Usage: python -m aerosim_b200.build [--force]
 
 Translation units and their floating-point contracts:
-  lbm_fast.cu   FP32-arithmetic step kernels, FMA contraction allowed
+  lbm_fast.cu   storage-type dispatch of the FP32-arithmetic step kernels
+  lbm_fast_<s>.cu  FP32-arithmetic step kernels per storage type, FMA contraction allowed
   lbm_exact.cu  FP64 kernels mirroring the reference's rounding: -fmad=false
   voxelize.cu   FP64 BVH voxelizer, bit-exact flags and links: -fmad=false
   engine.cu     C-ABI host layer
@@ -30,6 +31,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
           "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", CSRC, "-I", INCLUDE]
 UNITS = {
     "lbm_fast.cu": [],
+    "lbm_fast_f32.cu": [],
+    "lbm_fast_f16s.cu": [],
+    "lbm_fast_bf16s.cu": [],
     "lbm_exact.cu": ["-fmad=false"],
     "voxelize.cu": ["-fmad=false"],
     "engine.cu": [],
@@ -84,7 +88,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             raise RuntimeError(f"nvcc failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
         return r.stderr
 
-    with cf.ThreadPoolExecutor(max_workers=min(4, os.cpu_count() or 1)) as ex:
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         for msg in ex.map(run, jobs):
             if ptxas_info and msg:
                 print(msg)

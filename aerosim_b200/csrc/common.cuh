@@ -61,6 +61,9 @@ constexpr float F16S_INV_SCALE = 1.0f / 32768.0f;
 // pending mean-density rescale folded into the load; corr_s = corr / 2^15).
 struct StoreF32 {
   using T = float;
+  // FP32-collision output in the storage domain: value = kOutScale * h + kOutW * w_d
+  static constexpr float kOutScale = 1.0f, kOutW = 1.0f;
+  __device__ __forceinline__ static T store(float v) { return v; }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
     return fmaf(v, corr, -wf_of(d));
   }
@@ -71,6 +74,8 @@ struct StoreF32 {
 };
 struct StoreF64 {
   using T = double;
+  static constexpr float kOutScale = 1.0f, kOutW = 1.0f;
+  __device__ __forceinline__ static T store(float v) { return (double)v; }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
     return (float)(v * (double)corr - w64_of(d));
   }
@@ -81,6 +86,8 @@ struct StoreF64 {
 };
 struct StoreF16S {
   using T = __half;
+  static constexpr float kOutScale = F16S_SCALE, kOutW = 0.0f;
+  __device__ __forceinline__ static T store(float v) { return __float2half_rn(v); }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float corr_s) {
     return fmaf(__half2float(v), corr_s, wf_of(d) * (corr - 1.0f));
   }
@@ -91,6 +98,8 @@ struct StoreF16S {
 };
 struct StoreBF16S {
   using T = __nv_bfloat16;
+  static constexpr float kOutScale = 1.0f, kOutW = 0.0f;
+  __device__ __forceinline__ static T store(float v) { return __float2bfloat16_rn(v); }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
     return fmaf(__bfloat162float(v), corr, wf_of(d) * (corr - 1.0f));
   }
@@ -100,18 +109,43 @@ struct StoreBF16S {
   __device__ __forceinline__ static T raw_of_f(double f, int d) { return raw_of_h((float)(f - (double)wf_of(d)), d); }
 };
 
-// Solver memory layout.  Populations: plane d starts at d * plane; within a plane the
-// x-rows (iy, iz) are `pitch` elements apart (pitch = nx rounded up to 16, so every
-// row starts on a 16-byte boundary for the bulk copies).  The cell-class array uses
-// the same row pitch in bytes.
+// Storage order of the directions inside a row block ("slots"): directions that pull
+// from the same source row (same c_y, c_z) are adjacent, so one bulk copy brings all
+// of them.  Groups: (0,0): 0 1 2 | (1,0): 3 7 10 | (-1,0): 4 8 9 | (0,1): 5 11 14 |
+// (0,-1): 6 12 13 | (1,1): 15 | (-1,-1): 16 | (1,-1): 17 | (-1,1): 18.
+__host__ __device__ constexpr int slot_of(int d) {
+  return d <= 3 ? d : d == 4 ? 6 : d == 5 ? 9 : d == 6 ? 12 : d == 7 ? 4 : d == 8 ? 7 : d == 9 ? 8
+       : d == 10 ? 5 : d == 11 ? 10 : d == 12 ? 13 : d == 13 ? 14 : d == 14 ? 11 : d;
+}
+constexpr int kGroups = 9;
+__host__ __device__ constexpr int group_first(int g) { return g < 5 ? 3 * g : 10 + g; }
+__host__ __device__ constexpr int group_count(int g) { return g < 5 ? 3 : 1; }
+__host__ __device__ constexpr int group_cy(int g) {
+  return g == 1 || g == 5 || g == 7 ? 1 : g == 2 || g == 6 || g == 8 ? -1 : 0;
+}
+__host__ __device__ constexpr int group_cz(int g) {
+  return g == 3 || g == 5 || g == 8 ? 1 : g == 4 || g == 6 || g == 7 ? -1 : 0;
+}
+
+// Population memory layout.  Element (d, x, row) of a lattice with rows = ny * nz
+// x-rows lives at  row * rstride + slot(d) * dstride + x.
+//   solver (grouped = 1): row blocks -- the 19 direction rows of one x-row are
+//     contiguous, dstride = pitch, rstride = 19 * pitch, pitch = nx rounded up to 32
+//     (so each row starts on a 16-byte boundary and the 3-row groups are one copy);
+//   reference order (grouped = 0): SoA f[d * N + cell] as the reference stores it,
+//     dstride = plane = N, rstride = pitch = nx.
+// The cell-class array of the solver has one byte per cell with the same pitch.
 struct Layout {
-  long long plane;  // elements per direction plane
-  int pitch;        // elements per x-row
+  long long plane;    // elements per direction over the lattice (19 * plane in all)
+  long long rstride;  // elements between consecutive x-rows of one direction
+  long long dstride;  // elements between consecutive slots of one x-row
+  int pitch;          // elements per x-row
   int nx, ny, nz;
-  __host__ __device__ long long row_of(long long cell) const { return cell / nx; }
+  int grouped;
+  __host__ __device__ int slot(int d) const { return grouped ? slot_of(d) : d; }
   __host__ __device__ long long at(int d, long long cell) const {
     const long long r = cell / nx;
-    return (long long)d * plane + r * pitch + (cell - r * nx);
+    return r * rstride + (long long)slot(d) * dstride + (cell - r * nx);
   }
   __host__ __device__ long long cls_at(long long cell) const {
     const long long r = cell / nx;
@@ -122,8 +156,23 @@ struct Layout {
 __host__ inline Layout make_layout(int nx, int ny, int nz) {
   Layout L;
   L.nx = nx; L.ny = ny; L.nz = nz;
-  L.pitch = (nx + 15) / 16 * 16;
+  L.pitch = (nx + 31) / 32 * 32;
   L.plane = (long long)ny * nz * L.pitch;
+  L.dstride = L.pitch;
+  L.rstride = 19LL * L.pitch;
+  L.grouped = 1;
+  return L;
+}
+
+// The reference's own SoA order (dense, unpadded).
+__host__ inline Layout make_reference_layout(int nx, int ny, int nz) {
+  Layout L;
+  L.nx = nx; L.ny = ny; L.nz = nz;
+  L.pitch = nx;
+  L.plane = (long long)nx * ny * nz;
+  L.dstride = L.plane;
+  L.rstride = nx;
+  L.grouped = 0;
   return L;
 }
 

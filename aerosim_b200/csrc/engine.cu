@@ -128,6 +128,7 @@ int configure_step(aerosim_engine* h) {
   const size_t eb = precision_bytes(h->cfg.precision);
   const dim3 block(kStepThreads, 1, 1);
   StepArgs dummy{};
+  dummy.L = L;  // the kernel instance depends on the row pitch
   const char* env = getenv("AEROSIM_STAGES");
   const int forced = env ? atoi(env) : 0;
   int best_s = 0, best_occ = 0;
@@ -254,10 +255,7 @@ int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[
     const long long nn = (long long)nearv.size();
     if ((long long)19 * nl.plane >= (1LL << 32))
       return fail(h, AEROSIM_ERR_ARG, "lattice too large for 32-bit population offsets");
-    auto off = [&](int d, long long c) -> uint32_t {
-      const long long r = c / ng.nx;
-      return (uint32_t)((long long)d * nl.plane + r * nl.pitch + (c - r * ng.nx));
-    };
+    auto off = [&](int d, long long c) -> uint32_t { return (uint32_t)nl.at(d, c); };
     std::vector<NearLink> links(19 * std::max<long long>(nn, 1));
     for (long long t = 0; t < nn; ++t) {
       const long long cell = nearv[t];

@@ -26,8 +26,8 @@ size_t precision_bytes(int precision) {
 cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
                         cudaStream_t s, int* occ, int* launches) {
   switch (precision) {
-    case AEROSIM_PREC_F32_MIRROR: return step_entry<StoreF32, MODE_MIRROR>(a, block, grid, smem, s, occ, launches);
-    case AEROSIM_PREC_F64: return step_entry<StoreF64, MODE_F64>(a, block, grid, smem, s, occ, launches);
+    case AEROSIM_PREC_F32_MIRROR: return step_dispatch<StoreF32, MODE_MIRROR>(a, block, grid, smem, s, occ, launches);
+    case AEROSIM_PREC_F64: return step_dispatch<StoreF64, MODE_F64>(a, block, grid, smem, s, occ, launches);
     default: return launch_step_fast(precision, a, block, grid, smem, s, occ, launches);
   }
 }

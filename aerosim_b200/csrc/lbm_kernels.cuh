@@ -259,6 +259,112 @@ __device__ __forceinline__ void collide_f32(float (&h)[19], float& r, float& ux,
   }
 }
 
+// Approximate reciprocal and square root (one MUFU operation each); the FP32 path is
+// held to a tolerance against the oracle, not to its rounding.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// The same regularized collision as collide_f32 written as one second-order Hermite
+// expansion, which needs fewer operations per direction:
+//   f*_i = w_i [rho + 3 c_i.j + 4.5 Q_i : X],   X = rho u u + (1 - omega) Pi^neq,
+// and, with Pi^neq = S - (rho - 1)/3 I - rho u u (S = sum cc h),
+//   X = (S - (rho - 1)/3 I) - omega Pi^neq.
+// With B = rho - 1 - 1.5 tr X the deviation is h_i = w_i (B + 4.5 c_i c_i : X + 3 c_i.j).
+// rho and u are the clamped, Mach-limited values the reference forms its equilibrium
+// from (lbmCpuReference.ts:233-262), j = rho u.  The results are written back into
+// h[] already in the storage domain of S (kOutScale * h + kOutW * w), the storage's
+// scale and rest weight folded into the per-direction constants.
+template <class S>
+__device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux, float& uy, float& uz,
+                                             float tau0, float k_smag) {
+  constexpr float OS = S::kOutScale, OW = S::kOutW;
+  constexpr float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
+  float s[9], t[9];
+#pragma unroll
+  for (int p = 0; p < 9; ++p) {
+    s[p] = h[2 * p + 1] + h[2 * p + 2];
+    t[p] = h[2 * p + 1] - h[2 * p + 2];
+  }
+  const float dr = h[0] + ((s[0] + s[1]) + (s[2] + s[3]) + ((s[4] + s[5]) + (s[6] + s[7])) + s[8]);
+  const float jx = (t[0] + t[3]) + (t[4] + t[5]) + t[6];
+  const float jy = (t[1] + t[3]) - t[4] + (t[7] + t[8]);
+  const float jz = (t[2] + t[5]) - t[6] + (t[7] - t[8]);
+  const float sxx = (s[0] + s[3]) + (s[4] + s[5]) + s[6];
+  const float syy = (s[1] + s[3]) + (s[4] + s[7]) + s[8];
+  const float szz = (s[2] + s[5]) + (s[6] + s[7]) + s[8];
+  const float sxy = s[3] - s[4], sxz = s[5] - s[6], syz = s[7] - s[8];
+
+  r = fmaxf(0.5f, fminf(1.8f, 1.0f + dr));
+  if (dr != dr) r = dr;  // keep NaN visible like Math.min / Math.max
+  const float ir = rcp_approx(r);
+  ux = jx * ir; uy = jy * ir; uz = jz * ir;
+  const float uSq0 = ux * ux + uy * uy + uz * uz;
+  if (uSq0 > 0.0484f) {  // Mach limiter |u| <= 0.22
+    const float sc = 0.22f * rsqrtf(uSq0);
+    ux *= sc; uy *= sc; uz *= sc;
+  }
+  const float drc = r - 1.0f;
+  const float d3 = drc * (1.0f / 3.0f);
+  const float jcx = r * ux, jcy = r * uy, jcz = r * uz;
+  const float dxx = sxx - d3, dyy = syy - d3, dzz = szz - d3;
+  const float pxx = fmaf(-jcx, ux, dxx), pyy = fmaf(-jcy, uy, dyy), pzz = fmaf(-jcz, uz, dzz);
+  const float pxy = fmaf(-jcx, uy, sxy), pxz = fmaf(-jcx, uz, sxz), pyz = fmaf(-jcy, uz, syz);
+  const float off = fmaf(pxy, pxy, fmaf(pxz, pxz, pyz * pyz));
+  const float pn = sqrt_approx(fmaf(pxx, pxx, fmaf(pyy, pyy, fmaf(pzz, pzz, 2.0f * off))));
+  const float tau = 0.5f * (tau0 + sqrt_approx(fmaf(tau0, tau0, k_smag * pn * ir)));
+  const float om = rcp_approx(fmaxf(0.5015f, fminf(1.95f, tau)));
+  const float xxx = fmaf(-om, pxx, dxx), xyy = fmaf(-om, pyy, dyy), xzz = fmaf(-om, pzz, dzz);
+  const float xxy = fmaf(-om, pxy, sxy), xxz = fmaf(-om, pxz, sxz), xyz = fmaf(-om, pyz, syz);
+  const float B = fmaf(-1.5f, (xxx + xyy) + xzz, drc);
+  const float b = OW == 0.0f ? OS * B : fmaf(OS, B, OW);
+  h[0] = w0 * b;
+  // faces +-a: w1 (B + 4.5 X_aa +- 3 j_a)
+  const float b1 = w1 * b;
+  constexpr float kf = OS * 4.5f * w1, of = OS * 3.0f * w1;
+  {
+    const float E = fmaf(kf, xxx, b1), O = of * jcx;
+    h[1] = E + O; h[2] = E - O;
+  }
+  {
+    const float E = fmaf(kf, xyy, b1), O = of * jcy;
+    h[3] = E + O; h[4] = E - O;
+  }
+  {
+    const float E = fmaf(kf, xzz, b1), O = of * jcz;
+    h[5] = E + O; h[6] = E - O;
+  }
+  // edges +-(a +- b): w2 (B + 4.5 (X_aa + X_bb +- 2 X_ab) + 3 (j_a +- j_b))
+  const float b2 = w2 * b;
+  constexpr float ke = OS * 4.5f * w2, ke2 = OS * 9.0f * w2, oe = OS * 3.0f * w2;
+  const float qx = oe * jcx, qy = oe * jcy, qz = oe * jcz;
+  {
+    const float base = fmaf(ke, xxx + xyy, b2);
+    const float Ep = fmaf(ke2, xxy, base), Em = fmaf(-ke2, xxy, base);
+    const float Op = qx + qy, Om = qx - qy;
+    h[7] = Ep + Op; h[8] = Ep - Op; h[9] = Em + Om; h[10] = Em - Om;
+  }
+  {
+    const float base = fmaf(ke, xxx + xzz, b2);
+    const float Ep = fmaf(ke2, xxz, base), Em = fmaf(-ke2, xxz, base);
+    const float Op = qx + qz, Om = qx - qz;
+    h[11] = Ep + Op; h[12] = Ep - Op; h[13] = Em + Om; h[14] = Em - Om;
+  }
+  {
+    const float base = fmaf(ke, xyy + xzz, b2);
+    const float Ep = fmaf(ke2, xyz, base), Em = fmaf(-ke2, xyz, base);
+    const float Op = qy + qz, Om = qy - qz;
+    h[15] = Ep + Op; h[16] = Ep - Op; h[17] = Em + Om; h[18] = Em - Om;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // 1-D bulk-copy (TMA) and mbarrier helpers: global -> shared row copies whose
 // completion is counted in bytes on a shared-memory mbarrier.
@@ -317,29 +423,36 @@ __host__ __device__ inline int row_span(int nx) {  // threads along x (multiple 
 }
 __host__ __device__ inline int rows_per_item(int nx) { return (kConsumerWarps * 32) / row_span(nx); }
 
-// Dynamic shared memory of the step kernel: `stages` slots, each holding the 19
-// source row segments and the class bytes of the item's destination rows, plus a
-// full and an empty mbarrier per slot.
+// Dynamic shared memory of the step kernel, in order: a guard; the ring of `stages`
+// slots, each holding RY row blocks (19 slot rows of `pitch` elements, pulled from
+// their source rows); the class bytes of the slots' destination rows; a guard; a
+// full and an empty mbarrier per slot; the inlet tables ux_in[ny], uy_in[ny]; the
+// row coordinates [stages][RY]; per consumer warp an outlet scratch row of 20
+// floats; the per-lane direction table (c_x, c_y, c_z, w; slot) of the row-end cells.
 __host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem) {
   return (size_t)rows_per_item(L.nx) * (19 * (size_t)L.pitch * elem + (size_t)L.pitch);
 }
-// Guard bytes around the slots: the x-face cells read (and discard) one element
-// before the first row or past the end of a row.
 constexpr size_t kSmemGuard = 64;
 __host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem) {
-  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 * (size_t)stages + 16 +
-         2 * (size_t)L.ny * sizeof(double) + (size_t)stages * rows_per_item(L.nx) * sizeof(int2);
+  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 + 16 * (size_t)stages +
+         2 * (size_t)L.ny * sizeof(double) + (size_t)stages * rows_per_item(L.nx) * sizeof(int2) +
+         kConsumerWarps * 20 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int);
 }
 
 // ---------------------------------------------------------------------------
 // One launch per time step, main_kernel: a persistent CTA of 8 consumer warps, a
-// producer warp and a helper warp.  The producer streams x-rows into the shared
-// ring with bulk copies; the consumers walk the rows: pull, collide, wall
-// conditions (:375-429), inlet and outlet (:323-373), store.  Meanwhile the helper
-// warp takes the CTA's share of the near-wall cells (Bouzidi, :196-221; one lane
-// per cell from a link table built with the voxel grid).  A near-wall cell at
-// ix = 1 or nx-2 carries its row's inlet or outlet, which need its post-collision
-// values.  The last CTA takes the step's mean-density rescale decision (:431-455).
+// producer warp and a helper warp.  The producer streams row blocks into the shared
+// ring with bulk copies, one copy per group of directions that share a source row;
+// the consumers walk the rows: pull, collide, wall conditions (:375-429), inlet and
+// outlet (:323-373), store.  Meanwhile the helper warp takes the CTA's share of the
+// near-wall cells (Bouzidi, :196-221; one lane per cell from a link table built with
+// the voxel grid).  A near-wall cell at ix = 1 or nx-2 carries its row's inlet or
+// outlet, which need its post-collision values.  The last CTA takes the step's
+// mean-density rescale decision (:431-455).
+//
+// P is the row pitch when it is a compile-time constant (0: L.pitch at run time):
+// with a constant pitch every shared-memory load and global store of a cell is an
+// immediate offset from one base address.
 // ---------------------------------------------------------------------------
 
 // Near-wall link table: the value pulled along direction d is  A * p1 + B * p2  with
@@ -351,13 +464,10 @@ __host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, s
 // A and B are formed exactly as the reference forms them (lbmCpuReference.ts:211-220),
 // so A * p1 + B * p2 evaluates the same expression; with B = 0 it returns p1.
 struct NearLink {
-  uint32_t o1, o2;  // element offsets of p1, p2 (plane * direction + row * pitch + x)
+  uint32_t o1, o2;  // element offsets of p1, p2 (Layout::at)
   uint32_t d1, d2;  // their directions (the shifted codecs decode with w_d)
   double A, B;
 };
-
-// Shared-memory inlet tables appended after the ring: ux_in[ny], uy_in[ny].
-__host__ __device__ inline size_t step_inlet_bytes(const Layout& L) { return 2 * (size_t)L.ny * sizeof(double); }
 
 template <class S, int MODE>
 __device__ __forceinline__ void wall_feq(typename std::conditional<MODE == MODE_FAST, float, double>::type (&v)[19],
@@ -373,15 +483,15 @@ __device__ __forceinline__ void wall_feq(typename std::conditional<MODE == MODE_
 // front), collision, the deferred inlet / outlet of its row (ix = 1 or nx-2, from its
 // values before any wall condition), the wall condition when it applies, stores.
 // Returns the fixed-point density added to the step's sum; sets *nan on a NaN.
-template <class S, int MODE>
+template <class S, int MODE, int P>
 __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, double corr,
                                                const double* s_uxi, const double* s_uyi, int* nan) {
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
   using Mac = typename MacroOf<T>::type;
-  const Layout L = a.L;
-  const int nx = L.nx, ny = L.ny, nz = L.nz, pitch = L.pitch;
-  const long long plane = L.plane;
+  const Layout& L = a.L;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const int pitch = P ? P : L.pitch;
   const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
   T* __restrict__ fd = static_cast<T*>(a.fdst);
   long long add = 0;
@@ -389,8 +499,9 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
   const int ix = (int)(cell % nx);
   const long long row = cell / nx;
   const int iy = (int)(row % ny), iz = (int)(row / ny);
-  const long long pop_row = row * pitch;
-  const int flag = a.cls[pop_row + ix] & CLS_FLAG_MASK;
+  const long long cls_row = row * pitch;
+  T* const blk = fd + row * 19 * pitch;  // the row block of the destination row
+  const int flag = a.cls[cls_row + ix] & CLS_FLAG_MASK;
   const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
   auto resc = [&](double f) -> double {
     if constexpr (MODE == MODE_MIRROR) return (double)(float)(f * corr);
@@ -413,39 +524,41 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
     else collide_f64<MODE == MODE_MIRROR>(v, r, ux, uy, uz, a.tau0, a.k_smag);
     mr = (Mac)r; mx = (Mac)ux; my = (Mac)uy; mz = (Mac)uz;
   }
-  if (ix == 1 && (a.cls[pop_row] & CLS_FLAG_MASK) != CELL_SOLID) {
+  if (ix == 1 && (a.cls[cls_row] & CLS_FLAG_MASK) != CELL_SOLID) {
     // deferred inlet (:328-352)
     const long long ic = row * nx;
     const double uxi = s_uxi[iy], uyi = s_uyi[iy];
     const double ri = MODE == MODE_FAST ? (double)(0.85f * (float)mr + 0.15f) : 0.85 * (double)mr + 0.15 * 1.0;
-    T* out = fd + pop_row;
 #pragma unroll
     for (int d = 0; d < 19; ++d) {
-      if constexpr (MODE == MODE_FAST) out[d * plane] = S::raw_of_h(heq32(d, (float)ri, (float)uxi, (float)uyi, 0.f), d);
-      else out[d * plane] = S::raw_of_f(feq64(d, ri, uxi, uyi, 0.0), d);
+      if constexpr (MODE == MODE_FAST)
+        blk[slot_of(d) * pitch] = S::raw_of_h(heq32(d, (float)ri, (float)uxi, (float)uyi, 0.f), d);
+      else blk[slot_of(d) * pitch] = S::raw_of_f(feq64(d, ri, uxi, uyi, 0.0), d);
     }
     if (a.write_macro) {
       a.mux[ic] = (float)uxi; a.muy[ic] = (float)uyi; a.muz[ic] = 0.0f; a.mrho[ic] = (float)(Mac)ri;
     }
     add += rho_fixed((Mac)ri);
   }
-  if (ix == nx - 2 && (a.cls[pop_row + nx - 1] & CLS_FLAG_MASK) != CELL_SOLID) {
+  if (ix == nx - 2 && (a.cls[cls_row + nx - 1] & CLS_FLAG_MASK) != CELL_SOLID) {
     // deferred outlet (:354-371)
     const long long oc = row * nx + nx - 1;
-    T* out = fd + pop_row + nx - 1;
+    T* out = blk + nx - 1;
     Mac ro;
     if constexpr (MODE == MODE_FAST) {
       const float r2 = (float)mr * 0.85f + 0.15f;
 #pragma unroll
       for (int d = 0; d < 19; ++d)
-        out[d * plane] = S::raw_of_h(0.75f * v[d] + 0.25f * heq32(d, r2, (float)mx, (float)my, (float)mz), d);
+        out[slot_of(d) * pitch] =
+            S::raw_of_h(0.75f * v[d] + 0.25f * heq32(d, r2, (float)mx, (float)my, (float)mz), d);
       ro = (Mac)r2;
     } else {
       const double r2 = (double)mr * 0.85 + 1.0 * 0.15;
 #pragma unroll
       for (int d = 0; d < 19; ++d) {
         const double stored = S::f_of(S::raw_of_f(v[d], d), d);
-        out[d * plane] = S::raw_of_f(0.75 * stored + 0.25 * feq64(d, r2, (double)mx, (double)my, (double)mz), d);
+        out[slot_of(d) * pitch] =
+            S::raw_of_f(0.75 * stored + 0.25 * feq64(d, r2, (double)mx, (double)my, (double)mz), d);
       }
       ro = (Mac)r2;
     }
@@ -463,11 +576,11 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
     if (nz > 4 && (iz == 0 || iz == nz - 1)) mz = (Mac)0;
     wall_feq<S, MODE>(v, (double)mr, (double)mx, (double)my, (double)mz);
   }
-  T* out = fd + pop_row + ix;
+  T* out = blk + ix;
 #pragma unroll
   for (int d = 0; d < 19; ++d) {
-    if constexpr (MODE == MODE_FAST) out[d * plane] = S::raw_of_h(v[d], d);
-    else out[d * plane] = S::raw_of_f(v[d], d);
+    if constexpr (MODE == MODE_FAST) out[slot_of(d) * pitch] = S::raw_of_h(v[d], d);
+    else out[slot_of(d) * pitch] = S::raw_of_f(v[d], d);
   }
   if (a.write_macro) {
     a.mux[cell] = (float)mx; a.muy[cell] = (float)my; a.muz[cell] = (float)mz; a.mrho[cell] = (float)mr;
@@ -477,9 +590,132 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
   return add;
 }
 
-template <class S, int MODE>
+// Per-lane state of a consumer cell handed to the general path.
+struct CellCtx {
+  long long row;     // x-row of the warp's segment
+  int ix;            // cell index along x (may lie outside the row for idle lanes)
+  int iy, iz;
+  int cell_lo;       // cell of lane 0
+  int flag;
+  bool active, near;
+};
+
+// Consumer path of the double modes, with the reference's per-cell logic on the
+// pulled values v: collision, inlet / outlet (:323-373) inside the warp that holds the
+// row end, wall conditions (:375-429), stores.  Returns the fixed-point density added
+// to the step's sum.
+template <class S, int MODE, int P>
+__device__ __forceinline__ long long general_cells(const StepArgs& a, double (&v)[19], const CellCtx cc,
+                                                   const double* s_uxi, const double* s_uyi, int* my_nan) {
+  using T = typename S::T;
+  using Mac = typename MacroOf<T>::type;
+  const Layout& L = a.L;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const int pitch = P ? P : L.pitch;
+  T* __restrict__ fd = static_cast<T*>(a.fdst);
+  const int ix = cc.ix, iy = cc.iy, iz = cc.iz, flag = cc.flag, cell_lo = cc.cell_lo;
+  const bool active = cc.active, near = cc.near;
+  const bool solid = !active || flag == CELL_SOLID;
+  const bool xface = (ix == 0 || ix == nx - 1);
+  const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
+  const bool row_ok = cc.row < (long long)ny * nz;
+  const bool has_lo = row_ok && cell_lo <= 0 && 1 <= cell_lo + 31;
+  const bool has_hi = row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31;
+  T* const blk = fd + cc.row * 19 * pitch;
+  long long add = 0;
+
+  Mac mr, mx, my, mz;
+  {
+    double r, ux, uy, uz;
+    collide_f64<MODE == MODE_MIRROR>(v, r, ux, uy, uz, a.tau0, a.k_smag);
+    mr = (Mac)r; mx = (Mac)ux; my = (Mac)uy; mz = (Mac)uz;
+  }
+  bool done = active && !solid && !xface && !near;  // this lane stores its cell
+
+  // ---- inlet / outlet (:323-373), inside the warp that holds the row end ----
+  if (has_lo) {
+    const int src = 1 - cell_lo;
+    // rho at ix = 1 is 1 for a solid (:177); a near-wall ix = 1 defers the inlet
+    const double rho1 = __shfl_sync(0xffffffffu, solid ? 1.0 : (double)mr, src);
+    const int defer = __shfl_sync(0xffffffffu, (int)(near && !solid), src);
+    if (ix == 0 && !solid && !defer) {
+      const double uxi = s_uxi[iy], uyi = s_uyi[iy];
+      const double ri = 0.85 * rho1 + 0.15 * 1.0;
+#pragma unroll
+      for (int d = 0; d < 19; ++d) v[d] = feq64(d, ri, uxi, uyi, 0.0);
+      mr = (Mac)ri;
+      mx = (Mac)uxi; my = (Mac)uyi; mz = (Mac)0;
+      done = true;
+    }
+  }
+  if (has_hi) {
+    const int src = nx - 2 - cell_lo;
+    const int defer = __shfl_sync(0xffffffffu, (int)(near && !solid), src);
+    if (!defer) {
+      // the outlet reads fDst at nx-2 before the walls (:363): the stored value,
+      // or for a solid cell whatever fDst holds there (never written)
+      double send[19];
+      const bool stale = (ix == nx - 2) && solid;
+#pragma unroll
+      for (int d = 0; d < 19; ++d) {
+        if (stale) send[d] = S::f_of(blk[slot_of(d) * pitch + ix], d);
+        else send[d] = S::f_of(S::raw_of_f(v[d], d), d);
+      }
+      const double m0 = __shfl_sync(0xffffffffu, stale ? 1.0 : (double)mr, src);
+      const double m1 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)mx, src);
+      const double m2 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)my, src);
+      const double m3 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)mz, src);
+#pragma unroll
+      for (int d = 0; d < 19; ++d) send[d] = __shfl_sync(0xffffffffu, send[d], src);
+      if (ix == nx - 1 && !solid) {
+        const double ro = m0 * 0.85 + 1.0 * 0.15;
+#pragma unroll
+        for (int d = 0; d < 19; ++d) v[d] = 0.75 * send[d] + 0.25 * feq64(d, ro, m1, m2, m3);
+        mr = (Mac)ro;
+        mx = (Mac)m1; my = (Mac)m2; mz = (Mac)m3;
+        done = true;
+      }
+    }
+  }
+  // ---- wall conditions (:375-429): own moments, floor, ceiling, then sides ----
+  if (wall_row && done && !xface && flag == CELL_FLUID) {
+    if (iy == 0) {
+      if (a.ground_no_slip) { mx = (Mac)0; mz = (Mac)0; }
+      my = (Mac)0;
+    }
+    if (iy == ny - 1) my = (Mac)0;
+    if (nz > 4 && (iz == 0 || iz == nz - 1)) mz = (Mac)0;
+    wall_feq<S, MODE>(v, (double)mr, (double)mx, (double)my, (double)mz);
+  }
+  if (done) {
+    T* out = blk + ix;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::raw_of_f(v[d], d);
+    if (mr == mr) add += rho_fixed(mr);
+    else *my_nan = 1;
+  }
+  if (a.write_macro) {
+    const long long di = cc.row * nx + ix;
+    if (active && solid) {  // solid macro (:173-179)
+      a.mux[di] = 0.0f; a.muy[di] = 0.0f; a.muz[di] = 0.0f; a.mrho[di] = 1.0f;
+    } else if (done) {
+      a.mux[di] = (float)mx; a.muy[di] = (float)my; a.muz[di] = (float)mz; a.mrho[di] = (float)mr;
+    }
+  }
+  return add;
+}
+
+// Equilibrium deviation of a run-time direction (the lane-transposed row ends):
+// c = (c_x, c_y, c_z), w the float weight.
+__device__ __forceinline__ float heq_lane(const float4 c, float rho, float ux, float uy, float uz) {
+  const float cu = 3.0f * (c.x * ux + c.y * uy + c.z * uz);
+  const float uSq = ux * ux + uy * uy + uz * uz;
+  return c.w * ((rho - 1.0f) + rho * (cu + 0.5f * cu * cu - 1.5f * uSq));
+}
+
+template <class S, int MODE, int P>
 __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST_MIN_BLOCKS : 1)
-    main_kernel(const StepArgs a) {
+    main_kernel(const __grid_constant__ StepArgs a) {
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
   using Mac = typename MacroOf<T>::type;
@@ -488,9 +724,9 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
   __shared__ long long red[kConsumerWarps + 2];
   __shared__ int nan_flag;
 
-  const Layout L = a.L;
-  const int nx = L.nx, ny = L.ny, nz = L.nz, pitch = L.pitch;
-  const long long plane = L.plane;
+  const Layout& L = a.L;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const int pitch = P ? P : L.pitch;
   const int S_ = a.stages;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int shift = row_shift(nx), span = row_span(nx), RY = rows_per_item(nx);
@@ -506,18 +742,43 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
   uint64_t* empty = full + S_;
   double* s_uxi = reinterpret_cast<double*>(empty + S_);
   double* s_uyi = s_uxi + ny;
-  int2* s_row = reinterpret_cast<int2*>(s_uyi + ny);  // [S_][RY] (iy, iz) of the slot's rows
+  int2* s_row = reinterpret_cast<int2*>(s_uyi + ny);        // [S_][RY] (iy, iz) of the slot's rows
+  float* s_xo = reinterpret_cast<float*>(s_row + S_ * RY);  // [kConsumerWarps][20]
+  float4* s_dcw = reinterpret_cast<float4*>(
+      (reinterpret_cast<uintptr_t>(s_xo + kConsumerWarps * 20) + 15) & ~uintptr_t(15));  // [19]
+  int* s_dslot = reinterpret_cast<int*>(s_dcw + 19);                                     // [19]
 
   const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
   T* __restrict__ fd = static_cast<T*>(a.fdst);
 
+  // Consumer warps that own a row segment: RY rows of wpr warps.  When wpr does not
+  // divide the 8 consumer warps (row spans of 96, 160, 192, 224 threads) the
+  // remaining warps take no rows.
+  const int n_cons = RY * wpr;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S_; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kConsumerWarps);
+      mbar_init(&empty[s], n_cons);
     }
     nan_flag = 0;
     mbar_fence_init();
+  }
+  if (threadIdx.x < 19) {  // direction table of the lane-transposed row ends
+    const int d = threadIdx.x;
+    const int px = (1 << 1) | (1 << 7) | (1 << 9) | (1 << 11) | (1 << 13);
+    const int mx_ = (1 << 2) | (1 << 8) | (1 << 10) | (1 << 12) | (1 << 14);
+    const int py = (1 << 3) | (1 << 7) | (1 << 10) | (1 << 15) | (1 << 17);
+    const int my_ = (1 << 4) | (1 << 8) | (1 << 9) | (1 << 16) | (1 << 18);
+    const int pz = (1 << 5) | (1 << 11) | (1 << 14) | (1 << 15) | (1 << 18);
+    const int mz_ = (1 << 6) | (1 << 12) | (1 << 13) | (1 << 16) | (1 << 17);
+    const float w = d == 0 ? 1.0f / 3.0f : (d <= 6 ? 1.0f / 18.0f : 1.0f / 36.0f);
+    s_dcw[d] = make_float4((float)(((px >> d) & 1) - ((mx_ >> d) & 1)), (float)(((py >> d) & 1) - ((my_ >> d) & 1)),
+                           (float)(((pz >> d) & 1) - ((mz_ >> d) & 1)), w);
+    int sl = d;
+#pragma unroll
+    for (int e = 0; e < 19; ++e)
+      if (e == d) sl = slot_of(e);
+    s_dslot[d] = sl;
   }
   // inlet velocity per iy (:334-342), evaluated once per CTA
   for (int i = threadIdx.x; i < ny; i += blockDim.x) {
@@ -539,72 +800,84 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
     const double corr = a.st->apply[pslot] ? a.st->corr[pslot] : 1.0;
     int my_nan = 0;
     for (long long t = (long long)blockIdx.x * 32 + lane; t < a.n_near; t += (long long)gridDim.x * 32)
-      my_sum += near_cell<S, MODE>(a, t, corr, s_uxi, s_uyi, &my_nan);
+      my_sum += near_cell<S, MODE, P>(a, t, corr, s_uxi, s_uyi, &my_nan);
     if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
   } else if (warp == kProducerWarp) {
-    // ---------------- producer warp ----------------
-    if (lane == 0) {
-      const uint32_t row_bytes = (uint32_t)(pitch * sizeof(T));
-      int issued = 0;
-      for (int j = 0; j < my_count; ++j) {
-        const int s = j % S_;
-        if (j >= S_ && !mbar_wait(&empty[s], (uint32_t)(((j / S_) - 1) & 1), kWaitLimit)) {
+    // ---------------- producer warp: lanes issue the copies of an item in parallel ----------------
+    const uint32_t slot_bytes = (uint32_t)(pitch * sizeof(T));
+    int issued = 0;
+    int s = 0;
+    uint32_t ph = 0;  // parity of the slot's current fill
+    long long r0 = (long long)blockIdx.x * RY;
+    const long long r_step = (long long)gridDim.x * RY;
+    for (int j = 0; j < my_count; ++j, r0 += r_step) {
+      if (j >= S_) {  // the slot's previous fill must have been consumed
+        const bool ok = mbar_wait(&empty[s], ph ^ 1u, kWaitLimit);
+        if (!__any_sync(0xffffffffu, ok)) {
           failed = true;
           break;
         }
-        const long long r0 = (blockIdx.x + (long long)j * gridDim.x) * RY;
-        const int nr = (int)(rows - r0 < RY ? rows - r0 : RY);
+      }
+      const int nr = (int)(rows - r0 < RY ? rows - r0 : RY);
+      if (lane == 0) {
         // row coordinates for the consumers, published by the arrive below
         for (int yy = 0; yy < nr; ++yy) {
           const int r = (int)(r0 + yy);
           s_row[s * RY + yy] = make_int2(r % ny, r / ny);
         }
-        mbar_arrive_expect_tx(&full[s], (uint32_t)nr * (19u * row_bytes + (uint32_t)pitch));
-        for (int yy = 0; yy < nr; ++yy) {
-          const int2 yz = s_row[s * RY + yy];
-          const int iy = yz.x, iz = yz.y;
-          const long long r = r0 + yy;
-          T* dst = spop + ((size_t)s * RY + yy) * 19 * pitch;
-#pragma unroll
-          for (int d = 0; d < 19; ++d) {
-            const long long sr =
-                clampi(iy - cy_of(d), 0, ny - 1) + (long long)ny * clampi(iz - cz_of(d), 0, nz - 1);
-            bulk_load(dst + (size_t)d * pitch, fs + d * plane + sr * pitch, row_bytes, &full[s]);
-          }
-          bulk_load(scls + ((size_t)s * RY + yy) * pitch, a.cls + r * pitch, (uint32_t)pitch, &full[s]);
-        }
-        issued = j + 1;
+        mbar_arrive_expect_tx(&full[s], (uint32_t)nr * (19u * slot_bytes + (uint32_t)pitch));
       }
-      if (failed) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
-      // No copy may still be in flight when the CTA exits: wait (bounded) for the
-      // last phase issued into every slot; completed phases return at once.
-      for (int s = 0; s < S_ && s < issued; ++s) {
-        const int last = s + ((issued - 1 - s) / S_) * S_;
-        mbar_wait(&full[s], (uint32_t)((last / S_) & 1), kWaitLimit);
+      __syncwarp();
+      // copy c: row yy = c / 10, part g = c % 10 (9 direction groups, then the class bytes)
+      for (int c = lane; c < nr * 10; c += 32) {
+        const int yy = c / 10, g = c - yy * 10;
+        const long long r = r0 + yy;
+        if (g < kGroups) {
+          const int2 yz = s_row[s * RY + yy];
+          const long long sr =
+              clampi(yz.x - group_cy(g), 0, ny - 1) + (long long)ny * clampi(yz.y - group_cz(g), 0, nz - 1);
+          const int first = group_first(g);
+          bulk_load(spop + ((size_t)(s * RY + yy) * 19 + first) * pitch, fs + (sr * 19 + first) * pitch,
+                    (uint32_t)group_count(g) * slot_bytes, &full[s]);
+        } else {
+          bulk_load(scls + (size_t)(s * RY + yy) * pitch, a.cls + r * pitch, (uint32_t)pitch, &full[s]);
+        }
+      }
+      issued = j + 1;
+      if (++s == S_) { s = 0; ph ^= 1u; }
+    }
+    if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
+    // No copy may still be in flight when the CTA exits: wait (bounded) for the
+    // last phase issued into every slot; completed phases return at once.
+    if (lane == 0) {
+      for (int k = 0; k < S_ && k < issued; ++k) {
+        const int last = k + ((issued - 1 - k) / S_) * S_;
+        mbar_wait(&full[k], (uint32_t)((last / S_) & 1), kWaitLimit);
       }
     }
-  } else {
+  } else if (warp < n_cons) {
     // ---------------- consumer warps ----------------
     const int pslot = (a.step_index + 1) & 1;  // pending rescale of the previous step
-    const int apply = a.st->apply[pslot];
-    const double corr = apply ? a.st->corr[pslot] : 1.0;
+    const double corr = a.st->apply[pslot] ? a.st->corr[pslot] : 1.0;
     const float corrf = (float)corr;
     const float corrf_s = corrf * F16S_INV_SCALE;
     const int ry = warp / wpr;
     const int nchunks = (nx + shift + span - 1) / span;
     int my_nan = 0;
+    int s = 0;
+    uint32_t ph = 0;
+    int seg = warp % wpr;  // the row-end segments rotate over the warps of a row
+    long long row = (long long)blockIdx.x * RY + ry;
+    const long long row_step = (long long)gridDim.x * RY;
 
-    for (int j = 0; j < my_count; ++j) {
-      const int s = j % S_;
-      if (!mbar_wait(&full[s], (uint32_t)((j / S_) & 1), kWaitLimit)) {
-        failed = true;
-        break;
+    for (int j = 0; j < my_count; ++j, row += row_step) {
+      {
+        const bool ok = mbar_wait(&full[s], ph, kWaitLimit);
+        if (!__any_sync(0xffffffffu, ok)) {
+          failed = true;
+          break;
+        }
       }
-      // The row-end warps carry the inlet and outlet: rotate the segment each warp
-      // takes from item to item so that extra work is spread over all warps.
-      const int seg = (warp % wpr + j) % wpr;
-      const int xslot0 = seg * 32 + lane;
-      const long long row = (blockIdx.x + (long long)j * gridDim.x) * RY + ry;
       const bool row_ok = row < rows;
       int iy = 0, iz = 0;
       if (row_ok) {
@@ -612,28 +885,23 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
         iy = yz.x;
         iz = yz.y;
       }
-      const T* sp = spop + ((size_t)s * RY + ry) * 19 * pitch;
-      const uint8_t* sc = scls + ((size_t)s * RY + ry) * pitch;
+      const T* sp = spop + (size_t)(s * RY + ry) * 19 * pitch;
+      const uint8_t* sc = scls + (size_t)(s * RY + ry) * pitch;
       const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
-      const long long dense_row = row * nx;
-      const long long pop_row = row * pitch;
 
       for (int c = 0; c < nchunks; ++c) {
-        const int ix = xslot0 + c * span - shift;
+        const int cell_lo = c * span + seg * 32 - shift;  // cell of lane 0
+        const int ix = cell_lo + lane;
         const bool active = row_ok && ix >= 0 && ix < nx;
         const int lx = (ix >= 0 && ix < nx) ? ix : 1;  // lanes outside the row read cell 1
         const uint8_t cl = sc[lx];
         const int flag = cl & CLS_FLAG_MASK;
-        const bool solid = !active || flag == CELL_SOLID;
-        const bool xface = (ix == 0 || ix == nx - 1);
         const bool near = (cl & CLS_NEAR) != 0;
         Real v[19];
-        // ---- pull-stream (lbmCpuReference.ts:189-231) from the staged rows.  Every
-        // lane loads and collides; x faces, near-wall cells and solids overwrite or
-        // discard the result. ----
+        // ---- pull-stream (lbmCpuReference.ts:189-231) from the staged rows ----
 #pragma unroll
         for (int d = 0; d < 19; ++d) {
-          const T raw = sp[d * pitch + lx - cx_of(d)];
+          const T raw = sp[slot_of(d) * pitch + lx - cx_of(d)];
           if constexpr (MODE == MODE_FAST) v[d] = S::h_scaled(raw, d, corrf, corrf_s);
           else if constexpr (MODE == MODE_MIRROR) v[d] = (double)(float)(S::f_of(raw, d) * corr);
           else v[d] = S::f_of(raw, d) * corr;
@@ -642,113 +910,114 @@ __global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
         }
-        Mac mr, mx, my, mz;
-        {
-          Real r, ux, uy, uz;
-          if constexpr (MODE == MODE_FAST) collide_f32(v, r, ux, uy, uz, (float)a.tau0, (float)a.k_smag);
-          else collide_f64<MODE == MODE_MIRROR>(v, r, ux, uy, uz, a.tau0, a.k_smag);
-          mr = (Mac)r; mx = (Mac)ux; my = (Mac)uy; mz = (Mac)uz;
-        }
-        bool done = active && !solid && !xface && !near;  // this lane stores its cell
 
-        // ---- inlet / outlet (:323-373), inside the warp that holds the row end ----
-        const int cell_lo = c * span + seg * 32 - shift;  // cell of lane 0
-        if (row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
-          const int src = 1 - cell_lo;
-          // rho at ix = 1 is 1 for a solid (:177); a near-wall ix = 1 defers the inlet
-          const double rho1 = __shfl_sync(0xffffffffu, solid ? 1.0 : (double)mr, src);
-          const int defer = __shfl_sync(0xffffffffu, (int)(near && !solid), src);
-          if (ix == 0 && !solid && !defer) {
-            const double uxi = s_uxi[iy], uyi = s_uyi[iy];
-            if constexpr (MODE == MODE_FAST) {
-              const float ri = 0.85f * (float)rho1 + 0.15f;
-#pragma unroll
-              for (int d = 0; d < 19; ++d) v[d] = heq32(d, ri, (float)uxi, (float)uyi, 0.f);
-              mr = (Mac)ri;
-            } else {
-              const double ri = 0.85 * rho1 + 0.15 * 1.0;
-#pragma unroll
-              for (int d = 0; d < 19; ++d) v[d] = feq64(d, ri, uxi, uyi, 0.0);
-              mr = (Mac)ri;
-            }
-            mx = (Mac)uxi; my = (Mac)uyi; mz = (Mac)0;
-            done = true;
-          }
-        }
-        if (row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31) {
-          const int src = nx - 2 - cell_lo;
-          const int defer = __shfl_sync(0xffffffffu, (int)(near && !solid), src);
-          if (!defer) {
-            // the outlet reads fDst at nx-2 before the walls (:363): the stored value,
-            // or for a solid cell whatever fDst holds there (never written)
-            Real send[19];
-            const bool stale = (ix == nx - 2) && solid;
-#pragma unroll
-            for (int d = 0; d < 19; ++d) {
-              if (stale) {
-                const double f = S::f_of(fd[d * plane + pop_row + ix], d);
-                send[d] = MODE == MODE_FAST ? (Real)(f - (double)wf_of(d)) : (Real)f;
-              } else if constexpr (MODE == MODE_FAST) {
-                send[d] = v[d];
-              } else {
-                send[d] = S::f_of(S::raw_of_f(v[d], d), d);
+        if constexpr (MODE == MODE_FAST) {
+          // ---- FP32 path: every lane collides its cell; near-wall cells are left to
+          // the helper warp and solids are never written.  The inlet and outlet cells
+          // of the row are written lane-transposed (lane d writes direction d), the
+          // wall rows replace the result by the equilibrium of the cell's moments. ----
+          T* const blk = fd + row * 19 * pitch;
+          const bool own = active && flag != CELL_SOLID && !near && ix != 0 && ix != nx - 1;
+          float r, ux, uy, uz;
+          collide_fast<S>(v, r, ux, uy, uz, (float)a.tau0, (float)a.k_smag);  // v: storage domain
+          if (row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
+            // inlet (:328-352): density of ix = 1 (1 for a solid, :177); a near-wall
+            // ix = 1 defers the inlet to the helper warp, a solid ix = 0 has none
+            const int c0 = __shfl_sync(0xffffffffu, (int)cl, -cell_lo);
+            const int c1 = __shfl_sync(0xffffffffu, (int)cl, 1 - cell_lo);
+            const float r1 = __shfl_sync(0xffffffffu, r, 1 - cell_lo);
+            const bool solid1 = (c1 & CLS_FLAG_MASK) == CELL_SOLID;
+            if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
+              const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
+              const float uxi = (float)s_uxi[iy], uyi = (float)s_uyi[iy];
+              if (lane < 19) {
+                const float4 cw = s_dcw[lane];
+                const float h = heq_lane(cw, ri, uxi, uyi, 0.0f);
+                blk[s_dslot[lane] * pitch] = S::store(fmaf(S::kOutScale, h, S::kOutW * cw.w));
+              }
+              if (lane == 0) {
+                if (ri == ri) my_sum += rho_fixed(ri);
+                else my_nan = 1;
+                if (a.write_macro) {
+                  const long long ic = row * nx;
+                  a.mux[ic] = uxi; a.muy[ic] = uyi; a.muz[ic] = 0.0f; a.mrho[ic] = ri;
+                }
               }
             }
-            const double m0 = __shfl_sync(0xffffffffu, stale ? 1.0 : (double)mr, src);
-            const double m1 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)mx, src);
-            const double m2 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)my, src);
-            const double m3 = __shfl_sync(0xffffffffu, stale ? 0.0 : (double)mz, src);
+          }
+          if (row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31) {
+            // outlet (:354-371) from the post-collision, pre-wall cell nx-2, or from
+            // what fDst holds there when nx-2 is solid; a near-wall nx-2 defers it
+            const int src = nx - 2 - cell_lo;
+            const int c2 = __shfl_sync(0xffffffffu, (int)cl, src);
+            const int c3 = __shfl_sync(0xffffffffu, (int)cl, src + 1);
+            const bool stale = (c2 & CLS_FLAG_MASK) == CELL_SOLID;
+            const float r2 = __shfl_sync(0xffffffffu, r, src);
+            const float ox = __shfl_sync(0xffffffffu, ux, src);
+            const float oy = __shfl_sync(0xffffffffu, uy, src);
+            const float oz = __shfl_sync(0xffffffffu, uz, src);
+            if ((c3 & CLS_FLAG_MASK) != CELL_SOLID && !((c2 & CLS_NEAR) && !stale)) {
+              float* xo = s_xo + warp * 20;
+              if (lane == src && !stale) {
 #pragma unroll
-            for (int d = 0; d < 19; ++d) send[d] = __shfl_sync(0xffffffffu, send[d], src);
-            if (ix == nx - 1 && !solid) {
-              if constexpr (MODE == MODE_FAST) {
-                const float ro = (float)m0 * 0.85f + 0.15f;
-#pragma unroll
-                for (int d = 0; d < 19; ++d)
-                  v[d] = 0.75f * send[d] + 0.25f * heq32(d, ro, (float)m1, (float)m2, (float)m3);
-                mr = (Mac)ro;
-              } else {
-                const double ro = m0 * 0.85 + 1.0 * 0.15;
-#pragma unroll
-                for (int d = 0; d < 19; ++d) v[d] = 0.75 * send[d] + 0.25 * feq64(d, ro, m1, m2, m3);
-                mr = (Mac)ro;
+                for (int d = 0; d < 19; ++d) xo[slot_of(d)] = v[d];
               }
-              mx = (Mac)m1; my = (Mac)m2; mz = (Mac)m3;
-              done = true;
+              __syncwarp();
+              const float ro = (stale ? 1.0f : r2) * 0.85f + 0.15f;
+              const float mx = stale ? 0.0f : ox, my = stale ? 0.0f : oy, mz = stale ? 0.0f : oz;
+              if (lane < 19) {
+                const float4 cw = s_dcw[lane];
+                const int sl = s_dslot[lane];
+                const float h = heq_lane(cw, ro, mx, my, mz);
+                const float prev = stale ? (float)blk[sl * pitch + nx - 2] : xo[sl];
+                blk[sl * pitch + nx - 1] =
+                    S::store(0.75f * prev + 0.25f * fmaf(S::kOutScale, h, S::kOutW * cw.w));
+              }
+              __syncwarp();
+              if (lane == 0) {
+                if (ro == ro) my_sum += rho_fixed(ro);
+                else my_nan = 1;
+                if (a.write_macro) {
+                  const long long oc = row * nx + nx - 1;
+                  a.mux[oc] = mx; a.muy[oc] = my; a.muz[oc] = mz; a.mrho[oc] = ro;
+                }
+              }
             }
           }
-        }
-        // ---- wall conditions (:375-429): own moments, floor, ceiling, then sides ----
-        if (wall_row) {
-          if (done && !xface && flag == CELL_FLUID) {
+          if (wall_row) {  // floor, ceiling, then sides (:375-429), fluid cells only
             if (iy == 0) {
-              if (a.ground_no_slip) { mx = (Mac)0; mz = (Mac)0; }
-              my = (Mac)0;
+              if (a.ground_no_slip) { ux = 0.0f; uz = 0.0f; }
+              uy = 0.0f;
             }
-            if (iy == ny - 1) my = (Mac)0;
-            if (nz > 4 && (iz == 0 || iz == nz - 1)) mz = (Mac)0;
-            wall_feq<S, MODE>(v, (double)mr, (double)mx, (double)my, (double)mz);
-          }
-        }
-        if (done) {
-          T* out = fd + pop_row + ix;
+            if (iy == ny - 1) uy = 0.0f;
+            if (nz > 4 && (iz == 0 || iz == nz - 1)) uz = 0.0f;
 #pragma unroll
-          for (int d = 0; d < 19; ++d) {
-            if constexpr (MODE == MODE_FAST) out[d * plane] = S::raw_of_h(v[d], d);
-            else out[d * plane] = S::raw_of_f(v[d], d);
+            for (int d = 0; d < 19; ++d) v[d] = fmaf(S::kOutScale, heq32(d, r, ux, uy, uz), S::kOutW * wf_of(d));
           }
-          if (mr == mr) my_sum += rho_fixed(mr);
-          else my_nan = 1;
-        }
-        if (a.write_macro) {
-          const long long di = dense_row + ix;
-          if (active && solid) {  // solid macro (:173-179)
-            a.mux[di] = 0.0f; a.muy[di] = 0.0f; a.muz[di] = 0.0f; a.mrho[di] = 1.0f;
-          } else if (done) {
-            a.mux[di] = (float)mx; a.muy[di] = (float)my; a.muz[di] = (float)mz; a.mrho[di] = (float)mr;
+          if (own) {
+            T* out = blk + ix;
+#pragma unroll
+            for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::store(v[d]);
+            if (r == r) my_sum += rho_fixed(r);
+            else my_nan = 1;
           }
+          if (a.write_macro && active) {
+            const long long di = row * nx + ix;
+            if (flag == CELL_SOLID) {  // solid macro (:173-179)
+              a.mux[di] = 0.0f; a.muy[di] = 0.0f; a.muz[di] = 0.0f; a.mrho[di] = 1.0f;
+            } else if (own) {
+              a.mux[di] = ux; a.muy[di] = uy; a.muz[di] = uz; a.mrho[di] = r;
+            }
+          }
+        } else {
+          CellCtx cc;
+          cc.row = row; cc.ix = ix; cc.iy = iy; cc.iz = iz; cc.cell_lo = cell_lo; cc.flag = flag;
+          cc.active = active; cc.near = near;
+          my_sum += general_cells<S, MODE, P>(a, v, cc, s_uxi, s_uyi, &my_nan);
         }
       }
+      if (++s == S_) { s = 0; ph ^= 1u; }
+      if (++seg == wpr) seg = 0;
     }
     if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
     if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);

@@ -105,7 +105,7 @@ extern "C" int aerosim_momentum_exchange_noalloc(const float* f, const uint8_t* 
   a.ticket = ticket;
   a.out = out;
   // the caller's dense layout f[d * N + idx]: a row pitch of nx, planes of N cells
-  a.L.nx = nx; a.L.ny = ny; a.L.nz = nz; a.L.pitch = nx; a.L.plane = N;
+  a.L = make_reference_layout(nx, ny, nz);
   a.B = boundary_count;
   a.prev_slot = -1;  // no pending rescale: the caller's populations are final
   forces_kernel<StoreF32, MODE_MIRROR><<<(unsigned)blocks, 256, 0, s>>>(a);

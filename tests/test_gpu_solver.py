@@ -208,10 +208,12 @@ def test_error_status_paths(gpu_engine_cls):
     assert eng.step_and_extract_slice(4) is None
 
 
-@pytest.mark.parametrize("dims", [(33, 12, 10), (97, 9, 7), (289, 6, 6), (3, 5, 6), (40, 20, 3), (64, 1, 8)])
+@pytest.mark.parametrize("dims", [(33, 12, 10), (97, 9, 7), (289, 6, 6), (3, 5, 6), (40, 20, 3), (64, 1, 8),
+                                  (65, 10, 8), (150, 8, 6), (200, 6, 6)])
 def test_mirror_bit_exact_awkward_lattices(gpu_engine_cls, oracle_mod, dims):
     """Row lengths that shift the thread mapping (nx = 1 mod 32), split a row over
-    several chunks (nx > 256), the minimum nx = 3, thin domains and ny = 1."""
+    several chunks (nx > 256), leave consumer warps without a row (row spans of 96,
+    160 and 224 threads), the minimum nx = 3, thin domains and ny = 1."""
     nx, ny, nz = dims
     r = max(1.0, min(ny, nz) / 4.0)
     c = meshes.lattice_center(nx, ny, nz, 1.0, (nx / 3, ny / 2 - 0.5, nz / 2 - 0.5))
@@ -224,3 +226,38 @@ def test_mirror_bit_exact_awkward_lattices(gpu_engine_cls, oracle_mod, dims):
     mg, mo = eng.read_macro(), orc.macro()
     for k in ("ux", "uy", "uz", "rho"):
         assert _bitdiff(mg[k], mo[k]) == 0, k
+
+
+@pytest.mark.parametrize("dims,xc", [((33, 12, 10), None), ((97, 9, 7), None), ((289, 6, 6), None), ((3, 5, 6), None),
+                                     ((40, 20, 3), None), ((64, 1, 8), None), ((150, 8, 6), None),
+                                     ((200, 6, 6), None), ((64, 16, 16), 1.0),
+                                     ((64, 16, 16), 62.0), ((65, 16, 16), 63.4), ((96, 16, 16), 0.2)])
+def test_fp32_awkward_lattices_and_bodies_at_the_faces(gpu_engine_cls, oracle_mod, dims, xc):
+    """FP32 path on the awkward row lengths, and with a body cut by the inlet or outlet
+    plane: solid and near-wall cells at ix = 0, 1, nx-2, nx-1 (inlet from a solid
+    neighbour's unit density, deferred inlet/outlet, outlet from a never-written
+    solid cell).  Populations within 1e-5 relative, macro fields within 1e-5."""
+    nx, ny, nz = dims
+    if xc is None:
+        r = max(1.0, min(ny, nz) / 4.0)
+        center = (nx / 3, ny / 2 - 0.5, nz / 2 - 0.5)
+    else:
+        r = 4.0
+        center = (xc, ny / 2 - 0.5, nz / 2 - 0.5)
+    c = meshes.lattice_center(nx, ny, nz, 1.0, center)
+    mesh = meshes.icosphere(r, c, 2) if nx > 8 and ny > 2 else (np.zeros((0, 3), np.float32), None)
+    case = cases.Case("awkward", nx, ny, nz, mesh, 0.05, 0.01, 0.1, 60)
+    vox, orc, eng = _pair(gpu_engine_cls, oracle_mod, case, "f32")
+    if xc is not None:
+        fl = vox.flags.reshape(nz, ny, nx)
+        edge = fl[:, :, [0, 1, nx - 2, nx - 1]]
+        assert (edge != 0).any(), "the body must reach the x faces"
+    orc.step(60, threads=1)
+    eng.step(60)
+    fg, fo = eng.read_populations().astype(np.float64), orc.f(0)
+    rel = np.abs(fg - fo) / np.maximum(np.abs(fo), 1e-12)
+    rel[np.tile(vox.flags == 1, 19)] = 0.0
+    assert rel.max() <= 1e-5, f"max relative population error {rel.max():.3e}"
+    mg, mo = eng.read_macro(), orc.macro()
+    for k in ("ux", "uy", "uz", "rho"):
+        assert np.allclose(mg[k], mo[k], rtol=1e-5, atol=1e-6), k
