@@ -24,10 +24,14 @@ namespace aerosim {
 
 enum { MODE_FAST = 0, MODE_MIRROR = 1, MODE_F64 = 2 };
 
-// Resident CTAs per SM the FP32 step kernel is register-budgeted for.
-#ifndef AEROSIM_FAST_MIN_BLOCKS
-#define AEROSIM_FAST_MIN_BLOCKS 2
-#endif
+// Resident CTAs per SM the step kernel is register-budgeted for.  FP32 storage gains
+// from a third CTA (more warps in flight per SM: 131 -> 121 us per step measured at
+// 256x128x128, with some spilling at 64 registers); the 16-bit storage kernels issue
+// more instructions per cell and lose more to spills at that budget, so they keep two.
+template <class S, int MODE>
+constexpr int step_min_blocks() {
+  return MODE != MODE_FAST ? 1 : (sizeof(typename S::T) == 4 ? 3 : 2);
+}
 
 struct NearLink;
 
@@ -714,7 +718,7 @@ __device__ __forceinline__ float heq_lane(const float4 c, float rho, float ux, f
 }
 
 template <class S, int MODE, int P>
-__global__ void __launch_bounds__(kStepThreads, MODE == MODE_FAST ? AEROSIM_FAST_MIN_BLOCKS : 1)
+__global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE>())
     main_kernel(const __grid_constant__ StepArgs a) {
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
