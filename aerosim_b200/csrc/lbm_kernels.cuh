@@ -486,18 +486,20 @@ __device__ __forceinline__ void wall_feq(typename std::conditional<MODE == MODE_
 // One near-wall cell: every pulled value from the link table (all loads issued up
 // front), collision, the deferred inlet / outlet of its row (ix = 1 or nx-2, from its
 // values before any wall condition), the wall condition when it applies, stores.
-// Returns the fixed-point density added to the step's sum; sets *nan on a NaN.
-template <class S, int MODE, int P>
-__device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, double corr,
-                                               const double* s_uxi, const double* s_uyi, int* nan) {
+// fsrc / fdst are the step's population buffers, inlet_u(iy) the inlet velocity
+// (double2) of row iy.  Returns the fixed-point density added to the step's sum; sets
+// *nan on a NaN.
+template <class S, int MODE, int P, class InletFn>
+__device__ __forceinline__ long long near_cell(const StepArgs& a, const void* fsrc, void* fdst, int write_macro,
+                                               long long t, double corr, InletFn inlet_u, int* nan) {
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
   using Mac = typename MacroOf<T>::type;
   const Layout& L = a.L;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const int pitch = P ? P : L.pitch;
-  const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
-  T* __restrict__ fd = static_cast<T*>(a.fdst);
+  const T* __restrict__ fs = static_cast<const T*>(fsrc);
+  T* __restrict__ fd = static_cast<T*>(fdst);
   long long add = 0;
   const long long cell = a.near_cells[t];
   const int ix = (int)(cell % nx);
@@ -531,7 +533,8 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
   if (ix == 1 && (a.cls[cls_row] & CLS_FLAG_MASK) != CELL_SOLID) {
     // deferred inlet (:328-352)
     const long long ic = row * nx;
-    const double uxi = s_uxi[iy], uyi = s_uyi[iy];
+    const double2 ui = inlet_u(iy);
+    const double uxi = ui.x, uyi = ui.y;
     const double ri = MODE == MODE_FAST ? (double)(0.85f * (float)mr + 0.15f) : 0.85 * (double)mr + 0.15 * 1.0;
 #pragma unroll
     for (int d = 0; d < 19; ++d) {
@@ -539,7 +542,7 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
         blk[slot_of(d) * pitch] = S::raw_of_h(heq32(d, (float)ri, (float)uxi, (float)uyi, 0.f), d);
       else blk[slot_of(d) * pitch] = S::raw_of_f(feq64(d, ri, uxi, uyi, 0.0), d);
     }
-    if (a.write_macro) {
+    if (write_macro) {
       a.mux[ic] = (float)uxi; a.muy[ic] = (float)uyi; a.muz[ic] = 0.0f; a.mrho[ic] = (float)(Mac)ri;
     }
     add += rho_fixed((Mac)ri);
@@ -566,7 +569,7 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
       }
       ro = (Mac)r2;
     }
-    if (a.write_macro) {
+    if (write_macro) {
       a.mux[oc] = (float)mx; a.muy[oc] = (float)my; a.muz[oc] = (float)mz; a.mrho[oc] = (float)ro;
     }
     add += rho_fixed(ro);
@@ -586,7 +589,7 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, long long t, d
     if constexpr (MODE == MODE_FAST) out[slot_of(d) * pitch] = S::raw_of_h(v[d], d);
     else out[slot_of(d) * pitch] = S::raw_of_f(v[d], d);
   }
-  if (a.write_macro) {
+  if (write_macro) {
     a.mux[cell] = (float)mx; a.muy[cell] = (float)my; a.muz[cell] = (float)mz; a.mrho[cell] = (float)mr;
   }
   if (mr == mr) add += rho_fixed(mr);
@@ -717,6 +720,124 @@ __device__ __forceinline__ float heq_lane(const float4 c, float rho, float ux, f
   return c.w * ((rho - 1.0f) + rho * (cu + 0.5f * cu * cu - 1.5f * uSq));
 }
 
+// One FP32-arithmetic consumer segment (32 cells of an x-row), shared by the
+// single-lattice and the batched step kernel.  v holds the lane's pulled deviations;
+// every lane collides its cell; near-wall cells are left to the near-wall pass and
+// solids are never written.  The inlet and outlet cells of the row are written
+// lane-transposed (lane d writes direction d) from the density of ix = 1 and the
+// post-collision, pre-wall values of nx-2 (shuffles and the 20-float row xo); the wall
+// rows replace a cell's result by the equilibrium of its moments.  inlet_u(iy) gives
+// the inlet velocity (float2) of row iy; m carries the macro outputs.
+struct SegGeom {
+  long long row;            // x-row of the segment
+  int nx, ny, nz, pitch;
+  int iy, iz, cell_lo, ix;  // row coordinates, cell of lane 0, this lane's cell
+  int flag;
+  bool row_ok, active, near, wall_row, ground_no_slip, write_macro;
+  uint8_t cl;               // this lane's class byte
+};
+
+template <class S, class InletFn>
+__device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __restrict__ fd, const SegGeom g,
+                                             float tau0, float k_smag, InletFn inlet_u, const StepArgs& m,
+                                             float* xo, const float4* s_dcw, const int* s_dslot, int lane,
+                                             long long& my_sum, int& my_nan) {
+  using T = typename S::T;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, pitch = g.pitch, cell_lo = g.cell_lo, ix = g.ix;
+  const long long row = g.row;
+  T* const blk = fd + row * 19 * pitch;
+  const bool own = g.active && g.flag != CELL_SOLID && !g.near && ix != 0 && ix != nx - 1;
+  float r, ux, uy, uz;
+  collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag);  // v: storage domain
+  if (g.row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
+    // inlet (:328-352): density of ix = 1 (1 for a solid, :177); a near-wall ix = 1
+    // defers the inlet to the near-wall pass, a solid ix = 0 has none
+    const int c0 = __shfl_sync(0xffffffffu, (int)g.cl, -cell_lo);
+    const int c1 = __shfl_sync(0xffffffffu, (int)g.cl, 1 - cell_lo);
+    const float r1 = __shfl_sync(0xffffffffu, r, 1 - cell_lo);
+    const bool solid1 = (c1 & CLS_FLAG_MASK) == CELL_SOLID;
+    if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
+      const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
+      const float2 ui = inlet_u(g.iy);
+      if (lane < 19) {
+        const float4 cw = s_dcw[lane];
+        const float h = heq_lane(cw, ri, ui.x, ui.y, 0.0f);
+        blk[s_dslot[lane] * pitch] = S::store(fmaf(S::kOutScale, h, S::kOutW * cw.w));
+      }
+      if (lane == 0) {
+        if (ri == ri) my_sum += rho_fixed(ri);
+        else my_nan = 1;
+        if (g.write_macro) {
+          const long long ic = row * nx;
+          m.mux[ic] = ui.x; m.muy[ic] = ui.y; m.muz[ic] = 0.0f; m.mrho[ic] = ri;
+        }
+      }
+    }
+  }
+  if (g.row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31) {
+    // outlet (:354-371) from the post-collision, pre-wall cell nx-2, or from what fDst
+    // holds there when nx-2 is solid; a near-wall nx-2 defers it
+    const int src = nx - 2 - cell_lo;
+    const int c2 = __shfl_sync(0xffffffffu, (int)g.cl, src);
+    const int c3 = __shfl_sync(0xffffffffu, (int)g.cl, src + 1);
+    const bool stale = (c2 & CLS_FLAG_MASK) == CELL_SOLID;
+    const float r2 = __shfl_sync(0xffffffffu, r, src);
+    const float ox = __shfl_sync(0xffffffffu, ux, src);
+    const float oy = __shfl_sync(0xffffffffu, uy, src);
+    const float oz = __shfl_sync(0xffffffffu, uz, src);
+    if ((c3 & CLS_FLAG_MASK) != CELL_SOLID && !((c2 & CLS_NEAR) && !stale)) {
+      if (lane == src && !stale) {
+#pragma unroll
+        for (int d = 0; d < 19; ++d) xo[slot_of(d)] = v[d];
+      }
+      __syncwarp();
+      const float ro = (stale ? 1.0f : r2) * 0.85f + 0.15f;
+      const float mx = stale ? 0.0f : ox, my = stale ? 0.0f : oy, mz = stale ? 0.0f : oz;
+      if (lane < 19) {
+        const float4 cw = s_dcw[lane];
+        const int sl = s_dslot[lane];
+        const float h = heq_lane(cw, ro, mx, my, mz);
+        const float prev = stale ? (float)blk[sl * pitch + nx - 2] : xo[sl];
+        blk[sl * pitch + nx - 1] = S::store(0.75f * prev + 0.25f * fmaf(S::kOutScale, h, S::kOutW * cw.w));
+      }
+      __syncwarp();
+      if (lane == 0) {
+        if (ro == ro) my_sum += rho_fixed(ro);
+        else my_nan = 1;
+        if (g.write_macro) {
+          const long long oc = row * nx + nx - 1;
+          m.mux[oc] = mx; m.muy[oc] = my; m.muz[oc] = mz; m.mrho[oc] = ro;
+        }
+      }
+    }
+  }
+  if (g.wall_row) {  // floor, ceiling, then sides (:375-429), fluid cells only
+    if (g.iy == 0) {
+      if (g.ground_no_slip) { ux = 0.0f; uz = 0.0f; }
+      uy = 0.0f;
+    }
+    if (g.iy == ny - 1) uy = 0.0f;
+    if (nz > 4 && (g.iz == 0 || g.iz == nz - 1)) uz = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) v[d] = fmaf(S::kOutScale, heq32(d, r, ux, uy, uz), S::kOutW * wf_of(d));
+  }
+  if (own) {
+    T* out = blk + ix;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::store(v[d]);
+    if (r == r) my_sum += rho_fixed(r);
+    else my_nan = 1;
+  }
+  if (g.write_macro && g.active) {
+    const long long di = row * nx + ix;
+    if (g.flag == CELL_SOLID) {  // solid macro (:173-179)
+      m.mux[di] = 0.0f; m.muy[di] = 0.0f; m.muz[di] = 0.0f; m.mrho[di] = 1.0f;
+    } else if (own) {
+      m.mux[di] = ux; m.muy[di] = uy; m.muz[di] = uz; m.mrho[di] = r;
+    }
+  }
+}
+
 template <class S, int MODE, int P>
 __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE>())
     main_kernel(const __grid_constant__ StepArgs a) {
@@ -804,7 +925,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE>())
     const double corr = a.st->apply[pslot] ? a.st->corr[pslot] : 1.0;
     int my_nan = 0;
     for (long long t = (long long)blockIdx.x * 32 + lane; t < a.n_near; t += (long long)gridDim.x * 32)
-      my_sum += near_cell<S, MODE, P>(a, t, corr, s_uxi, s_uyi, &my_nan);
+      my_sum += near_cell<S, MODE, P>(a, a.fsrc, a.fdst, a.write_macro, t, corr,
+                                      [&](int y) { return make_double2(s_uxi[y], s_uyi[y]); }, &my_nan);
     if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
   } else if (warp == kProducerWarp) {
     // ---------------- producer warp: lanes issue the copies of an item in parallel ----------------
@@ -916,103 +1038,14 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE>())
         }
 
         if constexpr (MODE == MODE_FAST) {
-          // ---- FP32 path: every lane collides its cell; near-wall cells are left to
-          // the helper warp and solids are never written.  The inlet and outlet cells
-          // of the row are written lane-transposed (lane d writes direction d), the
-          // wall rows replace the result by the equilibrium of the cell's moments. ----
-          T* const blk = fd + row * 19 * pitch;
-          const bool own = active && flag != CELL_SOLID && !near && ix != 0 && ix != nx - 1;
-          float r, ux, uy, uz;
-          collide_fast<S>(v, r, ux, uy, uz, (float)a.tau0, (float)a.k_smag);  // v: storage domain
-          if (row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
-            // inlet (:328-352): density of ix = 1 (1 for a solid, :177); a near-wall
-            // ix = 1 defers the inlet to the helper warp, a solid ix = 0 has none
-            const int c0 = __shfl_sync(0xffffffffu, (int)cl, -cell_lo);
-            const int c1 = __shfl_sync(0xffffffffu, (int)cl, 1 - cell_lo);
-            const float r1 = __shfl_sync(0xffffffffu, r, 1 - cell_lo);
-            const bool solid1 = (c1 & CLS_FLAG_MASK) == CELL_SOLID;
-            if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
-              const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
-              const float uxi = (float)s_uxi[iy], uyi = (float)s_uyi[iy];
-              if (lane < 19) {
-                const float4 cw = s_dcw[lane];
-                const float h = heq_lane(cw, ri, uxi, uyi, 0.0f);
-                blk[s_dslot[lane] * pitch] = S::store(fmaf(S::kOutScale, h, S::kOutW * cw.w));
-              }
-              if (lane == 0) {
-                if (ri == ri) my_sum += rho_fixed(ri);
-                else my_nan = 1;
-                if (a.write_macro) {
-                  const long long ic = row * nx;
-                  a.mux[ic] = uxi; a.muy[ic] = uyi; a.muz[ic] = 0.0f; a.mrho[ic] = ri;
-                }
-              }
-            }
-          }
-          if (row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31) {
-            // outlet (:354-371) from the post-collision, pre-wall cell nx-2, or from
-            // what fDst holds there when nx-2 is solid; a near-wall nx-2 defers it
-            const int src = nx - 2 - cell_lo;
-            const int c2 = __shfl_sync(0xffffffffu, (int)cl, src);
-            const int c3 = __shfl_sync(0xffffffffu, (int)cl, src + 1);
-            const bool stale = (c2 & CLS_FLAG_MASK) == CELL_SOLID;
-            const float r2 = __shfl_sync(0xffffffffu, r, src);
-            const float ox = __shfl_sync(0xffffffffu, ux, src);
-            const float oy = __shfl_sync(0xffffffffu, uy, src);
-            const float oz = __shfl_sync(0xffffffffu, uz, src);
-            if ((c3 & CLS_FLAG_MASK) != CELL_SOLID && !((c2 & CLS_NEAR) && !stale)) {
-              float* xo = s_xo + warp * 20;
-              if (lane == src && !stale) {
-#pragma unroll
-                for (int d = 0; d < 19; ++d) xo[slot_of(d)] = v[d];
-              }
-              __syncwarp();
-              const float ro = (stale ? 1.0f : r2) * 0.85f + 0.15f;
-              const float mx = stale ? 0.0f : ox, my = stale ? 0.0f : oy, mz = stale ? 0.0f : oz;
-              if (lane < 19) {
-                const float4 cw = s_dcw[lane];
-                const int sl = s_dslot[lane];
-                const float h = heq_lane(cw, ro, mx, my, mz);
-                const float prev = stale ? (float)blk[sl * pitch + nx - 2] : xo[sl];
-                blk[sl * pitch + nx - 1] =
-                    S::store(0.75f * prev + 0.25f * fmaf(S::kOutScale, h, S::kOutW * cw.w));
-              }
-              __syncwarp();
-              if (lane == 0) {
-                if (ro == ro) my_sum += rho_fixed(ro);
-                else my_nan = 1;
-                if (a.write_macro) {
-                  const long long oc = row * nx + nx - 1;
-                  a.mux[oc] = mx; a.muy[oc] = my; a.muz[oc] = mz; a.mrho[oc] = ro;
-                }
-              }
-            }
-          }
-          if (wall_row) {  // floor, ceiling, then sides (:375-429), fluid cells only
-            if (iy == 0) {
-              if (a.ground_no_slip) { ux = 0.0f; uz = 0.0f; }
-              uy = 0.0f;
-            }
-            if (iy == ny - 1) uy = 0.0f;
-            if (nz > 4 && (iz == 0 || iz == nz - 1)) uz = 0.0f;
-#pragma unroll
-            for (int d = 0; d < 19; ++d) v[d] = fmaf(S::kOutScale, heq32(d, r, ux, uy, uz), S::kOutW * wf_of(d));
-          }
-          if (own) {
-            T* out = blk + ix;
-#pragma unroll
-            for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::store(v[d]);
-            if (r == r) my_sum += rho_fixed(r);
-            else my_nan = 1;
-          }
-          if (a.write_macro && active) {
-            const long long di = row * nx + ix;
-            if (flag == CELL_SOLID) {  // solid macro (:173-179)
-              a.mux[di] = 0.0f; a.muy[di] = 0.0f; a.muz[di] = 0.0f; a.mrho[di] = 1.0f;
-            } else if (own) {
-              a.mux[di] = ux; a.muy[di] = uy; a.muz[di] = uz; a.mrho[di] = r;
-            }
-          }
+          SegGeom g;
+          g.row = row; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
+          g.iy = iy; g.iz = iz; g.cell_lo = cell_lo; g.ix = ix; g.flag = flag;
+          g.row_ok = row_ok; g.active = active; g.near = near; g.wall_row = wall_row;
+          g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro; g.cl = cl;
+          fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag,
+                          [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); }, a,
+                          s_xo + warp * 20, s_dcw, s_dslot, lane, my_sum, my_nan);
         } else {
           CellCtx cc;
           cc.row = row; cc.ix = ix; cc.iy = iy; cc.iz = iz; cc.cell_lo = cell_lo; cc.flag = flag;
