@@ -3,10 +3,10 @@ Bouzidi walls, FP64 momentum-exchange forces and the BVH voxelizer, exported by 
 C-ABI library libaerosim.so (include/aerosim.h) and mirrored here for Python hosts.
 """
 from ._native import AerosimError, PRECISIONS  # noqa: F401
-from .engine import (LBMEngine, VoxelGridResult, frontal_area, voxelize_mesh_to_lattice,  # noqa: F401
+from .engine import (LBMBatch, LBMEngine, VoxelGridResult, frontal_area, voxelize_mesh_to_lattice,  # noqa: F401
                      voxelizeMeshToLattice)
 from .forces import ForceConvergenceTracker, compute_normalized_force_coefficients  # noqa: F401
 
-__all__ = ["LBMEngine", "VoxelGridResult", "voxelize_mesh_to_lattice", "voxelizeMeshToLattice",
+__all__ = ["LBMEngine", "LBMBatch", "VoxelGridResult", "voxelize_mesh_to_lattice", "voxelizeMeshToLattice",
            "frontal_area", "ForceConvergenceTracker", "compute_normalized_force_coefficients",
            "AerosimError", "PRECISIONS"]

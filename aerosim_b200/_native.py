@@ -67,6 +67,11 @@ class Mass(C.Structure):
                 ("cumulative_rescale", C.c_double), ("rescale_count", C.c_int64)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("stages", C.c_int32), ("ctas_per_sm", C.c_int32), ("graph_steps", C.c_int32),
+                ("reserved", C.c_int32), ("ms_per_step", C.c_double)]
+
+
 _P = C.c_void_p
 _F32P = C.POINTER(C.c_float)
 _I32P = C.POINTER(C.c_int32)
@@ -96,6 +101,14 @@ SIGNATURES = {
     "aerosim_write_populations": ([_P, _P, C.c_int32], C.c_int),
     "aerosim_mass_stats": ([_P, C.POINTER(Mass)], C.c_int),
     "aerosim_last_step_timing": ([_P, _F64P, C.POINTER(C.c_int64)], C.c_int),
+    "aerosim_batch_create": ([C.POINTER(_P), C.c_int32, C.POINTER(_P)], C.c_int),
+    "aerosim_batch_destroy": ([_P], C.c_int),
+    "aerosim_batch_step": ([_P, C.c_int32], C.c_int),
+    "aerosim_batch_autotune": ([_P, C.c_int32, C.POINTER(BatchTuning)], C.c_int),
+    "aerosim_batch_set_tuning": ([_P, C.POINTER(BatchTuning)], C.c_int),
+    "aerosim_batch_get_tuning": ([_P, C.POINTER(BatchTuning)], C.c_int),
+    "aerosim_batch_last_timing": ([_P, _F64P, C.POINTER(C.c_int64)], C.c_int),
+    "aerosim_batch_cells": ([_P, C.POINTER(C.c_int64)], C.c_int),
     "aerosim_frontal_area": ([_F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P], C.c_int),
     "aerosim_momentum_exchange_noalloc": ([_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, C.c_int32, _P, _P],
                                           C.c_int),

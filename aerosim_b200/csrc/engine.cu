@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "engine_internal.h"
 #include "lbm_kernels.cuh"
+#include "lbm_batch.cuh"
 
 using namespace aerosim;
 
@@ -149,8 +150,7 @@ int configure_step(aerosim_engine* h) {
   h->block = block;
   h->stages = best_s;
   h->smem = step_smem_bytes(L, best_s, eb);
-  // the probes above raised the shared-memory attribute to their own sizes: set it
-  // (and the occupancy) for the chosen configuration
+  // the occupancy of the chosen configuration
   CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ, nullptr));
   h->occupancy = best_occ;
   const long long items = ((long long)L.ny * L.nz + rows_per_item(L.nx) - 1) / rows_per_item(L.nx);
@@ -813,6 +813,366 @@ int aerosim_frontal_area(const float* pos, int64_t nv, const int32_t* idx, int64
   long long covered = 0;
   for (uint16_t c : cover) covered += __builtin_popcount(c);
   *out = ((double)covered / ((double)res * res * 16)) * (span_y * span_z);
+  return AEROSIM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches: many engines stepped by one persistent launch per step.
+// ---------------------------------------------------------------------------
+struct aerosim_batch {
+  int device = 0;
+  int precision = 0;
+  std::vector<aerosim_engine*> eng;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  StepArgs* d_inst = nullptr;
+  void** d_bufs = nullptr;
+  long long* d_item_begin = nullptr;
+  long long* d_near_begin = nullptr;
+  unsigned long long* d_partials = nullptr;
+  unsigned int* d_ticket = nullptr;  // [2]
+  int* d_step = nullptr;
+  int* d_error = nullptr;
+  long long n_items = 0, n_near = 0, cells = 0;
+  long long slot_elems = 0, slot_cls = 0;
+  int pitch = 0;  // row pitch shared by all instances (0: they differ)
+  int num_sms = 148;
+  aerosim_batch_tuning tune{};
+  unsigned grid = 1;
+  size_t smem = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_len = 0;
+  int step = 0;
+  double last_ms = 0;
+  long long last_launches = 0;
+};
+
+namespace {
+
+int bfail(int code, const std::string& msg) { return fail(nullptr, code, msg); }
+
+#define BCU(x)                                                                            \
+  do {                                                                                    \
+    cudaError_t e_ = (x);                                                                 \
+    if (e_ != cudaSuccess) return bfail(AEROSIM_ERR_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+void batch_free(aerosim_batch* b) {
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  cudaFree(b->d_inst); cudaFree(b->d_bufs); cudaFree(b->d_item_begin); cudaFree(b->d_near_begin);
+  cudaFree(b->d_partials); cudaFree(b->d_ticket); cudaFree(b->d_step); cudaFree(b->d_error);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+// The solver arguments of every instance, from its engine's current configuration.
+int batch_upload_table(aerosim_batch* b) {
+  std::vector<StepArgs> t(b->eng.size());
+  for (size_t k = 0; k < b->eng.size(); ++k) {
+    const aerosim_engine* e = b->eng[k];
+    StepArgs& a = t[k];
+    a = StepArgs{};
+    a.cls = e->g.cls; a.bmap = e->g.bmap; a.q = e->g.q;
+    a.mux = e->mux; a.muy = e->muy; a.muz = e->muz; a.mrho = e->mrho;
+    a.abl = e->abl; a.sin_tab = e->sin_tab; a.st = e->st;
+    a.L = e->L; a.fluid_count = e->fluid_count;
+    a.near_cells = e->near_cells; a.n_near = e->n_near; a.links = e->links;
+    a.ground_no_slip = e->cfg.ground_no_slip;
+    a.u_inlet = e->cfg.u_inlet_lattice;
+    a.tau0 = 3.0 * e->cfg.nu_lattice + 0.5;
+    a.k_smag = 18.0 * M_SQRT2 * e->cfg.smagorinsky_cs * e->cfg.smagorinsky_cs;
+  }
+  BCU(cudaMemcpyAsync(b->d_inst, t.data(), t.size() * sizeof(StepArgs), cudaMemcpyHostToDevice, b->stream));
+  return AEROSIM_OK;
+}
+
+BatchArgs batch_args(const aerosim_batch* b, int write_macro) {
+  BatchArgs a{};
+  a.inst = b->d_inst; a.bufs = b->d_bufs; a.item_begin = b->d_item_begin; a.near_begin = b->d_near_begin;
+  a.partials = b->d_partials; a.ticket = b->d_ticket; a.step = b->d_step; a.error = b->d_error;
+  a.n_items = b->n_items; a.n_near = b->n_near; a.slot_elems = b->slot_elems; a.slot_cls = b->slot_cls;
+  a.n_inst = (int)b->eng.size(); a.stages = b->tune.stages; a.write_macro = write_macro;
+  return a;
+}
+
+// Launch shape of a tuning: the shared memory of its ring and the persistent grid, or
+// an error when the configuration does not fit.
+int batch_configure(aerosim_batch* b, const aerosim_batch_tuning& t, unsigned* grid, size_t* smem) {
+  if (t.stages < 2 || t.stages > 6 || t.ctas_per_sm < 1 || t.ctas_per_sm > 3 || t.graph_steps < 1)
+    return bfail(AEROSIM_ERR_ARG, "batch: tuning out of range (stages 2..6, ctas_per_sm 1..3, graph_steps >= 1)");
+  const size_t eb = precision_bytes(b->precision);
+  const size_t sm = batch_smem_bytes(b->slot_elems, b->slot_cls, t.stages, eb);
+  if (sm > 227 * 1024) return bfail(AEROSIM_ERR_ARG, "batch: the ring does not fit shared memory");
+  BatchArgs a = batch_args(b, 0);
+  a.stages = t.stages;
+  int occ = 0;
+  BCU(launch_batch(b->precision, a, b->pitch, 0, sm, b->stream, &occ));
+  if (occ < t.ctas_per_sm) return bfail(AEROSIM_ERR_ARG, "batch: fewer resident CTAs per SM than requested");
+  long long g = (long long)t.ctas_per_sm * b->num_sms;
+  if (g > b->n_items) g = b->n_items;
+  *grid = (unsigned)(g < 1 ? 1 : g);
+  *smem = sm;
+  return AEROSIM_OK;
+}
+
+int batch_apply_tuning(aerosim_batch* b, const aerosim_batch_tuning& t) {
+  unsigned grid = 0;
+  size_t smem = 0;
+  int rc = batch_configure(b, t, &grid, &smem);
+  if (rc) return rc;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->tune = t;
+  b->grid = grid;
+  b->smem = smem;
+  return AEROSIM_OK;
+}
+
+// Fresh flow in every instance and the batch's step counter at zero.
+int batch_reset(aerosim_batch* b) {
+  for (aerosim_engine* e : b->eng) {
+    BCU(cudaSetDevice(e->device));
+    if (do_reset(e)) return bfail(AEROSIM_ERR_CUDA, "batch: reset of an instance failed: " + e->err);
+  }
+  BCU(cudaSetDevice(b->device));
+  BCU(cudaMemsetAsync(b->d_step, 0, sizeof(int), b->stream));
+  BCU(cudaMemsetAsync(b->d_ticket, 0, 2 * sizeof(unsigned int), b->stream));
+  BCU(cudaMemsetAsync(b->d_error, 0, sizeof(int), b->stream));
+  BCU(cudaStreamSynchronize(b->stream));
+  b->step = 0;
+  return AEROSIM_OK;
+}
+
+// Enqueues n batched steps: replays of the captured graph of tune.graph_steps launches,
+// then single launches; the last step writes the macro fields.
+int batch_enqueue(aerosim_batch* b, int n, long long* launches) {
+  const int G = b->tune.graph_steps;
+  int done = 0;
+  if (G > 1 && n >= G) {
+    if (!b->graph) {
+      cudaGraph_t g = nullptr;
+      BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t le = cudaSuccess;
+      for (int i = 0; i < G && le == cudaSuccess; ++i) {
+        const BatchArgs a = batch_args(b, i == G - 1 ? 1 : 0);
+        le = launch_batch(b->precision, a, b->pitch, b->grid, b->smem, b->stream, nullptr);
+      }
+      const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+      if (le != cudaSuccess || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return bfail(AEROSIM_ERR_CUDA, std::string("batch: graph capture failed: ") +
+                                           cudaGetErrorString(le != cudaSuccess ? le : ce));
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        b->graph = nullptr;
+        return bfail(AEROSIM_ERR_CUDA, std::string("batch: graph instantiation failed: ") + cudaGetErrorString(ie));
+      }
+      b->graph_len = G;
+    }
+    for (; done + G <= n; done += G) {
+      BCU(cudaGraphLaunch(b->graph, b->stream));
+      *launches += G;
+    }
+  }
+  for (; done < n; ++done) {
+    const BatchArgs a = batch_args(b, done == n - 1 ? 1 : 0);
+    BCU(launch_batch(b->precision, a, b->pitch, b->grid, b->smem, b->stream, nullptr));
+    *launches += 1;
+  }
+  return AEROSIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batch** out) {
+  if (!out) return bfail(AEROSIM_ERR_ARG, "batch_create: out is NULL");
+  *out = nullptr;
+  if (!engines || n < 1 || n > kMaxBatch) return bfail(AEROSIM_ERR_ARG, "batch_create: 1..64 engines required");
+  for (int k = 0; k < n; ++k) {
+    const aerosim_engine* e = engines[k];
+    if (!e) return bfail(AEROSIM_ERR_ARG, "batch_create: NULL engine");
+    if (!e->have_grid || !e->f[0]) return bfail(AEROSIM_ERR_STATE, "batch_create: an engine has no voxel grid");
+    if (e->device != engines[0]->device) return bfail(AEROSIM_ERR_ARG, "batch_create: engines on different devices");
+    if (e->cfg.precision != engines[0]->cfg.precision)
+      return bfail(AEROSIM_ERR_ARG, "batch_create: engines with different precisions");
+    for (int j = 0; j < k; ++j)
+      if (engines[j] == e) return bfail(AEROSIM_ERR_ARG, "batch_create: an engine appears twice");
+  }
+  const int prec = engines[0]->cfg.precision;
+  if (prec != AEROSIM_PREC_F32 && prec != AEROSIM_PREC_F16S && prec != AEROSIM_PREC_BF16S)
+    return bfail(AEROSIM_ERR_ARG, "batch_create: batches run the F32, F16S and BF16S precisions");
+  aerosim_batch* b = new (std::nothrow) aerosim_batch();
+  if (!b) return bfail(AEROSIM_ERR_NOMEM, "batch_create: out of host memory");
+  b->device = engines[0]->device;
+  b->precision = prec;
+  b->eng.assign(engines, engines + n);
+  b->num_sms = engines[0]->num_sms;
+  auto bail = [&](int rc) {
+    std::string msg = aerosim_last_error(nullptr);
+    batch_free(b);
+    delete b;
+    return bfail(rc, msg);
+  };
+  cudaError_t e = cudaSetDevice(b->device);
+  std::vector<long long> item_begin(n + 1, 0), near_begin(n + 1, 0);
+  std::vector<void*> bufs(2 * (size_t)n);
+  int pitch = engines[0]->L.pitch;
+  for (int k = 0; k < n; ++k) {
+    const aerosim_engine* en = engines[k];
+    const Layout& L = en->L;
+    const int RY = rows_per_item(L.nx);
+    const long long rows = (long long)L.ny * L.nz;
+    item_begin[k + 1] = item_begin[k] + (rows + RY - 1) / RY;
+    near_begin[k + 1] = near_begin[k] + en->n_near;
+    bufs[2 * k] = en->f[0];
+    bufs[2 * k + 1] = en->f[1];
+    b->slot_elems = std::max<long long>(b->slot_elems, (long long)RY * 19 * L.pitch);
+    b->slot_cls = std::max<long long>(b->slot_cls, (long long)RY * L.pitch);
+    b->cells += en->g.N;
+    if (L.pitch != pitch) pitch = 0;
+  }
+  b->pitch = (pitch == 64 || pitch == 128 || pitch == 192 || pitch == 256) ? pitch : 0;
+  b->n_items = item_begin[n];
+  b->n_near = near_begin[n];
+  const size_t part = (size_t)3 * b->num_sms * n;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_inst, n * sizeof(StepArgs));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_bufs, 2 * n * sizeof(void*));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_item_begin, (n + 1) * sizeof(long long));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_near_begin, (n + 1) * sizeof(long long));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_partials, part * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_ticket, 2 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_step, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_error, sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_bufs, bufs.data(), bufs.size() * sizeof(void*), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_item_begin, item_begin.data(), item_begin.size() * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_near_begin, near_begin.data(), near_begin.size() * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    bfail(AEROSIM_ERR_CUDA, std::string("batch_create: ") + cudaGetErrorString(e));
+    return bail(AEROSIM_ERR_CUDA);
+  }
+  int rc = batch_reset(b);
+  if (!rc) rc = batch_upload_table(b);
+  if (rc) return bail(rc);
+  // default launch: the most resident CTAs per SM that a 3-slot ring allows (at least a
+  // 2-slot ring), 20 launches per graph
+  aerosim_batch_tuning t{3, 3, 20, 0, 0.0};
+  rc = AEROSIM_ERR_ARG;
+  for (int stages = 3; stages >= 2 && rc; --stages)
+    for (int c = 3; c >= 1 && rc; --c) {
+      t.stages = stages;
+      t.ctas_per_sm = c;
+      rc = batch_apply_tuning(b, t);
+    }
+  if (rc) return bail(rc);
+  *out = b;
+  return AEROSIM_OK;
+}
+
+int aerosim_batch_destroy(aerosim_batch* b) {
+  if (!b) return AEROSIM_OK;
+  batch_free(b);
+  delete b;
+  return AEROSIM_OK;
+}
+
+int aerosim_batch_step(aerosim_batch* b, int32_t n) {
+  if (!b) return bfail(AEROSIM_ERR_ARG, "batch_step: NULL batch");
+  if (n < 0) return bfail(AEROSIM_ERR_ARG, "batch_step: negative step count");
+  if ((long long)b->step + n > 0x7fffffffLL) return bfail(AEROSIM_ERR_ARG, "batch_step: step index overflow");
+  BCU(cudaSetDevice(b->device));
+  for (aerosim_engine* e : b->eng) BCU(cudaStreamSynchronize(e->stream));
+  int rc = batch_upload_table(b);
+  if (rc) return rc;
+  long long launches = 0;
+  BCU(cudaEventRecord(b->ev0, b->stream));
+  rc = batch_enqueue(b, n, &launches);
+  if (rc) return rc;
+  BCU(cudaEventRecord(b->ev1, b->stream));
+  int dev_err = 0;
+  BCU(cudaMemcpyAsync(&dev_err, b->d_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BCU(cudaStreamSynchronize(b->stream));
+  float ms = 0.f;
+  BCU(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  b->last_ms = ms;
+  b->last_launches = launches;
+  b->step += n;
+  for (aerosim_engine* e : b->eng) {
+    e->step_index = b->step;
+    e->cur = b->step & 1;
+  }
+  if (dev_err) return bfail(AEROSIM_ERR_DEVICE, "batch_step: the shared-memory pipeline timed out (device error flag set)");
+  return AEROSIM_OK;
+}
+
+int aerosim_batch_autotune(aerosim_batch* b, int32_t steps_per_trial, aerosim_batch_tuning* out) {
+  if (!b) return bfail(AEROSIM_ERR_ARG, "batch_autotune: NULL batch");
+  if (steps_per_trial < 1) return bfail(AEROSIM_ERR_ARG, "batch_autotune: steps_per_trial must be positive");
+  BCU(cudaSetDevice(b->device));
+  const aerosim_batch_tuning keep = b->tune;
+  aerosim_batch_tuning best = keep;
+  best.ms_per_step = 1e300;
+  for (int stages = 2; stages <= 6; ++stages)
+    for (int c = 1; c <= 3; ++c) {
+      aerosim_batch_tuning t{stages, c, 1, 0, 0.0};
+      if (batch_apply_tuning(b, t) != AEROSIM_OK) continue;  // does not fit: skip
+      int rc = aerosim_batch_step(b, 2);
+      if (!rc) rc = aerosim_batch_step(b, steps_per_trial);
+      if (rc) return rc;
+      const double per = b->last_ms / steps_per_trial;
+      if (per < best.ms_per_step) {
+        best = t;
+        best.ms_per_step = per;
+      }
+    }
+  best.graph_steps = keep.graph_steps;
+  int rc = batch_apply_tuning(b, best);
+  if (rc) return rc;
+  b->tune.ms_per_step = best.ms_per_step;
+  rc = batch_reset(b);
+  if (rc) return rc;
+  if (out) *out = b->tune;
+  return AEROSIM_OK;
+}
+
+int aerosim_batch_set_tuning(aerosim_batch* b, const aerosim_batch_tuning* t) {
+  if (!b || !t) return bfail(AEROSIM_ERR_ARG, "batch_set_tuning: NULL argument");
+  BCU(cudaSetDevice(b->device));
+  return batch_apply_tuning(b, *t);
+}
+
+int aerosim_batch_get_tuning(aerosim_batch* b, aerosim_batch_tuning* out) {
+  if (!b || !out) return bfail(AEROSIM_ERR_ARG, "batch_get_tuning: NULL argument");
+  *out = b->tune;
+  return AEROSIM_OK;
+}
+
+int aerosim_batch_last_timing(aerosim_batch* b, double* ms, int64_t* kernel_launches) {
+  if (!b) return bfail(AEROSIM_ERR_ARG, "batch_last_timing: NULL batch");
+  if (ms) *ms = b->last_ms;
+  if (kernel_launches) *kernel_launches = b->last_launches;
+  return AEROSIM_OK;
+}
+
+int aerosim_batch_cells(aerosim_batch* b, int64_t* out) {
+  if (!b || !out) return bfail(AEROSIM_ERR_ARG, "batch_cells: NULL argument");
+  *out = b->cells;
   return AEROSIM_OK;
 }
 

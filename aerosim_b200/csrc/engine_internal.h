@@ -9,6 +9,7 @@ namespace aerosim {
 
 struct StepArgs;
 struct ForceArgs;
+struct BatchArgs;
 
 // A voxel grid resident on the device (VoxelGridResult, voxelizer.ts:19-59).
 struct DevGrid {
@@ -42,6 +43,10 @@ size_t precision_bytes(int precision);
 // attribute) for this block and dynamic shared-memory size.
 cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s,
                         int* occ, int* launches);
+// One batched step (FP32-arithmetic precisions only); pitch: the instances' common row
+// pitch or 0.  occ != nullptr: occupancy query as for launch_step.
+cudaError_t launch_batch(int precision, const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
+                         int* occ);
 cudaError_t launch_forces(int precision, const ForceArgs& a, unsigned grid, cudaStream_t s);
 cudaError_t launch_classify(const uint8_t* flags, uint8_t* cls, const Layout& L, cudaStream_t s);
 cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, float* mux, float* muy,

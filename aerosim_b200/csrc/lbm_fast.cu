@@ -1,4 +1,4 @@
-// Storage-type dispatch of the FP32-arithmetic step kernels (lbm_fast_<storage>.cu).
+// Storage-type dispatch of the FP32-arithmetic step and batch kernels (lbm_fast_<storage>.cu).
 #include "common.cuh"
 #include "engine_internal.h"
 #include "../../include/aerosim.h"
@@ -11,6 +11,23 @@ cudaError_t launch_step_fast_f16s(const StepArgs& a, dim3 block, unsigned grid, 
                                   int* occ, int* launches);
 cudaError_t launch_step_fast_bf16s(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s,
                                    int* occ, int* launches);
+
+cudaError_t launch_batch_fast_f32(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
+                                  int* occ);
+cudaError_t launch_batch_fast_f16s(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
+                                   int* occ);
+cudaError_t launch_batch_fast_bf16s(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
+                                    int* occ);
+
+cudaError_t launch_batch(int precision, const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
+                         int* occ) {
+  switch (precision) {
+    case AEROSIM_PREC_F32: return launch_batch_fast_f32(b, pitch, grid, smem, s, occ);
+    case AEROSIM_PREC_F16S: return launch_batch_fast_f16s(b, pitch, grid, smem, s, occ);
+    case AEROSIM_PREC_BF16S: return launch_batch_fast_bf16s(b, pitch, grid, smem, s, occ);
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 cudaError_t launch_step_fast(int precision, const StepArgs& a, dim3 block, unsigned grid, size_t smem,
                              cudaStream_t s, int* occ, int* launches) {

@@ -1,10 +1,27 @@
-// Launch helper shared by the kernel translation units: the step kernel uses
-// dynamic shared memory above 48 KB, so its attribute is raised before the
-// occupancy query that sizes the persistent grid.
+// Launch helpers shared by the kernel translation units: the step kernels use
+// dynamic shared memory above 48 KB, so their limit is raised before the occupancy
+// query that sizes the persistent grid.
 #pragma once
 #include "lbm_kernels.cuh"
+#include "lbm_batch.cuh"
 
 namespace aerosim {
+
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in maximum.  The
+// limit belongs to the kernel, not to a launch, so engines that share a kernel instance
+// with different ring sizes must never lower it below what another engine launches with.
+// (The maximum is the opt-in per-block size less the kernel's static shared memory.)
+template <class K>
+cudaError_t raise_smem_limit(K k) {
+  int dev = 0, mx = 0;
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, mx - (int)fa.sharedSizeBytes);
+  return e;
+}
 
 // One time step: a single main_kernel launch.  Returns the number of launches in
 // *launches.
@@ -13,7 +30,7 @@ cudaError_t step_entry(const StepArgs& a, dim3 block, unsigned grid, size_t smem
                        int* launches) {
   auto k = main_kernel<S, MODE, P>;
   if (occ) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = raise_smem_limit(k);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, (int)(block.x * block.y), smem);
   }
@@ -42,6 +59,31 @@ cudaError_t step_dispatch(const StepArgs& a, dim3 block, unsigned grid, size_t s
     }
   }
   return step_entry<S, MODE, 0>(a, block, grid, smem, s, occ, launches);
+}
+
+// One step of a batch (batch_kernel).  pitch: the row pitch shared by every instance,
+// or 0 when the instances differ (the kernel then reads each instance's pitch).
+template <class S, int P>
+cudaError_t batch_entry(const BatchArgs& b, unsigned grid, size_t smem, cudaStream_t s, int* occ) {
+  auto k = batch_kernel<S, P>;
+  if (occ) {
+    cudaError_t e = raise_smem_limit(k);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, kStepThreads, smem);
+  }
+  k<<<grid, kStepThreads, smem, s>>>(b);
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t batch_dispatch(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s, int* occ) {
+  switch (pitch) {
+    case 64: return batch_entry<S, 64>(b, grid, smem, s, occ);
+    case 128: return batch_entry<S, 128>(b, grid, smem, s, occ);
+    case 192: return batch_entry<S, 192>(b, grid, smem, s, occ);
+    case 256: return batch_entry<S, 256>(b, grid, smem, s, occ);
+    default: return batch_entry<S, 0>(b, grid, smem, s, occ);
+  }
 }
 
 }  // namespace aerosim

@@ -308,3 +308,66 @@ class LBMEngine:
     stepAndExtractSlice = step_and_extract_slice
     resetFlow = reset_flow
     getStepCount = get_step_count
+
+
+class LBMBatch:
+    """Many wind-tunnel instances stepped together: one persistent kernel launch per
+    step over the rows of all instances, runs of steps replayed from a CUDA graph
+    (aerosim_batch_*).  `engines` are LBMEngine objects with voxel grids and the same
+    FP32-arithmetic precision; creating the batch resets their flows.  Each engine's
+    readouts (forces, macro field, populations, mass stats) follow the batch's steps."""
+
+    def __init__(self, engines: list[LBMEngine]):
+        self.lib = N.load()
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e._h.h for e in self.engines])
+        h = C.c_void_p()
+        N.check(self.lib.aerosim_batch_create(arr, len(self.engines), C.byref(h)))
+        self.h = h
+
+    def step(self, n: int = 1) -> None:
+        N.check(self.lib.aerosim_batch_step(self.h, int(n)))
+
+    def autotune(self, steps_per_trial: int = 20) -> dict:
+        """Times every launch configuration that fits, keeps the fastest and resets
+        the flows."""
+        t = N.BatchTuning()
+        N.check(self.lib.aerosim_batch_autotune(self.h, int(steps_per_trial), C.byref(t)))
+        return self._tuning_dict(t)
+
+    def set_tuning(self, stages: int, ctas_per_sm: int, graph_steps: int = 20) -> None:
+        t = N.BatchTuning(int(stages), int(ctas_per_sm), int(graph_steps), 0, 0.0)
+        N.check(self.lib.aerosim_batch_set_tuning(self.h, C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = N.BatchTuning()
+        N.check(self.lib.aerosim_batch_get_tuning(self.h, C.byref(t)))
+        return self._tuning_dict(t)
+
+    @staticmethod
+    def _tuning_dict(t) -> dict:
+        return {"stages": t.stages, "ctasPerSm": t.ctas_per_sm, "graphSteps": t.graph_steps,
+                "msPerStep": t.ms_per_step}
+
+    def last_step_timing(self) -> tuple[float, int]:
+        ms = C.c_double()
+        n = C.c_int64()
+        N.check(self.lib.aerosim_batch_last_timing(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    @property
+    def cells(self) -> int:
+        v = C.c_int64()
+        N.check(self.lib.aerosim_batch_cells(self.h, C.byref(v)))
+        return v.value
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.aerosim_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -189,6 +189,43 @@ int aerosim_momentum_exchange_noalloc(const float* f, const uint8_t* flags, cons
                                       const float* q, int64_t boundary_count, int32_t nx, int32_t ny,
                                       int32_t nz, double* out, void* stream);
 
+/* ---- batches: many tunnels in one launch --------------------------------- */
+
+/* A batch steps many wind-tunnel instances (angle-of-attack or specimen sweeps, uneven
+ * lattice sizes) together: every step is ONE persistent kernel launch over the rows of
+ * all instances, and runs of steps are replayed from a captured CUDA graph.  No
+ * counterpart in the reference, which runs one tunnel per browser page; the instances
+ * are ordinary engines, so every per-engine call (forces, macro field, populations,
+ * mass statistics) works on them between batch steps. */
+typedef struct aerosim_batch aerosim_batch;
+
+/* Launch configuration of a batch, chosen by aerosim_batch_autotune or set by hand. */
+typedef struct {
+  int32_t stages;        /* shared-memory ring slots per CTA (2..6) */
+  int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid (1..3) */
+  int32_t graph_steps;   /* launches per captured CUDA graph (1: no graph) */
+  int32_t reserved;
+  double ms_per_step;    /* autotune: measured time of one batched step */
+} aerosim_batch_tuning;
+
+/* engines: n (1..64) engines on one device, each with a voxel grid, all with the same
+ * FP32-arithmetic precision (F32, F16S or BF16S).  Resets the flow of every instance;
+ * the engines must outlive the batch and must not be stepped alone while it exists
+ * (per-engine reads are fine).  Errors: aerosim_last_error(NULL). */
+int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batch** out);
+int aerosim_batch_destroy(aerosim_batch* b);
+/* n steps of every instance; each engine's step count and readouts advance with it. */
+int aerosim_batch_step(aerosim_batch* b, int32_t n);
+/* Times every launch configuration that fits (ring depth x resident CTAs per SM) over
+ * steps_per_trial steps each, keeps the fastest, then resets every instance's flow. */
+int aerosim_batch_autotune(aerosim_batch* b, int32_t steps_per_trial, aerosim_batch_tuning* out);
+int aerosim_batch_set_tuning(aerosim_batch* b, const aerosim_batch_tuning* t);
+int aerosim_batch_get_tuning(aerosim_batch* b, aerosim_batch_tuning* out);
+/* Device time (CUDA events) and kernel launches of the last aerosim_batch_step call. */
+int aerosim_batch_last_timing(aerosim_batch* b, double* ms, int64_t* kernel_launches);
+/* Cells of all instances (the MLUPS numerator of one batched step). */
+int aerosim_batch_cells(aerosim_batch* b, int64_t* out);
+
 /* ---- host-side geometry inputs ------------------------------------------- */
 
 /* computeProjectedFrontalArea(geometry, worldMatrix, gridResolution),

@@ -261,3 +261,18 @@ def test_fp32_awkward_lattices_and_bodies_at_the_faces(gpu_engine_cls, oracle_mo
     mg, mo = eng.read_macro(), orc.macro()
     for k in ("ux", "uy", "uz", "rho"):
         assert np.allclose(mg[k], mo[k], rtol=1e-5, atol=1e-6), k
+
+
+def test_engines_sharing_a_kernel_with_different_rings(gpu_engine_cls, oracle_mod):
+    """Two engines whose lattices use the same kernel instance (same row pitch) but
+    different shared-memory rings step alternately: configuring the second must not
+    shrink the first one's shared-memory limit."""
+    engines = []
+    for dims in [(128, 24, 20), (120, 48, 24)]:
+        c = cases.Case("pair", *dims, (np.zeros((0, 3), np.float32), None), 0.05, 0.01, 0.1, 5)
+        _, orc, eng = _pair(gpu_engine_cls, oracle_mod, c, "f32")
+        engines.append(eng)
+    for _ in range(2):
+        for eng in engines:
+            eng.step(3)
+    assert [e.get_step_count() for e in engines] == [6, 6]
