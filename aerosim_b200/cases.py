@@ -76,6 +76,26 @@ def naca_wing(aoa_deg: float, nx: int, ny: int, nz: int, steps: int = 10000) -> 
                 steps, extra={"aoa_deg": aoa_deg})
 
 
+def naca_batch(n: int = 32, seed: int = 0, steps: int = 10000, span: float = 64.0) -> list[Case]:
+    """The batched sweep: `n` extruded NACA 0012 wings (chord 48 cells) at angles of
+    attack drawn uniformly from [-8, 22] degrees (numpy default_rng(seed)), on lattices
+    growing from 128x64x64 to 190x95x95 (nx = 128 + 2i, ny = nz = nx / 2); u = 0.06,
+    Re = 5e3 on the chord (nu = 5.76e-4), Cs = 0.1.  The span is min(span, nz - 8)
+    cells so that the wing tips stay 4 cells clear of the side walls on the narrowest
+    lattices (nz = 64)."""
+    rng = np.random.default_rng(seed)
+    aoa = rng.uniform(-8.0, 22.0, n)
+    out = []
+    for i in range(n):
+        nx = 128 + 2 * i
+        ny = nz = nx // 2
+        c = meshes.lattice_center(nx, ny, nz, 1.0, (nx / 3 - 0.5, ny / 2 - 0.5, nz / 2 - 0.5))
+        mesh = meshes.naca0012_wing(48.0, min(span, nz - 8.0), float(aoa[i]), c)
+        out.append(Case(f"naca0012_{aoa[i]:+.1f}deg_{nx}x{ny}x{nz}", nx, ny, nz, mesh, 0.06, 0.06 * 48 / 5e3,
+                        0.1, steps, extra={"aoa_deg": float(aoa[i])}))
+    return out
+
+
 def mesh_reference_quantities(mesh: meshes.Mesh, frontal_fn) -> tuple[float, float]:
     """(A_ref, L_ref): projected frontal area on the Y-Z plane at 512^2 (frontalArea.ts)
     and the streamwise bounding-box length (stlLoader.ts:231)."""

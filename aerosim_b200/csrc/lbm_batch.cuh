@@ -1,7 +1,8 @@
 // Batched step kernel: many wind-tunnel instances of uneven lattice sizes advance one
 // time step in ONE persistent launch.  The items (x-row groups) of all instances form
 // one flat work list; a CTA walks it with the producer / consumer / near-wall warp
-// roles of main_kernel, switching the instance's arguments per item.  Each instance
+// roles of main_kernel, switching the instance's arguments per item and dealing the
+// 32-cell segments of an item to the consumer warps cyclically.  Each instance
 // keeps its own mean-density rescale: CTAs write per-instance partial density sums and
 // the last CTA takes every instance's decision.  The step counter lives in device
 // memory and the ping-pong buffers are selected by its parity, so a CUDA graph of
@@ -191,8 +192,12 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
     }
   } else {
     // ---------------- consumer warps ----------------
+    // The 32-cell segments of an item (RY rows of `segs` segments) are dealt to the 8
+    // warps cyclically, starting where the previous item stopped, so every warp has
+    // work whatever the row length.  A warp releases the slot after its last load.
     int s = 0;
     uint32_t ph = 0;
+    int offset = 0;  // warp that takes segment 0 of the current item
     for (int j = 0; j < my_count; ++j) {
       {
         const bool ok = mbar_wait(&full[s], ph, kWaitLimit);
@@ -206,13 +211,15 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
       const StepArgs& ia = b.inst[k];
       const int nx = ia.L.nx, ny = ia.L.ny, nz = ia.L.nz;
       const int pitch = P ? P : ia.L.pitch;
-      const int shift = row_shift(nx), span = row_span(nx), RY = rows_per_item(nx);
-      const int wpr = span / 32;
-      const int ry = warp / wpr;
+      const int shift = row_shift(nx), RY = rows_per_item(nx);
+      const int segs = (nx + shift + 31) / 32;  // segments per row
       const long long rows = (long long)ny * nz;
-      const long long row = (gi - b.item_begin[k]) * RY + ry;
-      const bool row_ok = ry < RY && row < rows;
-      if (ry >= RY) {  // no row of this item for this warp: release the slot at once
+      const long long row0 = (gi - b.item_begin[k]) * RY;
+      const int nr = (int)(rows - row0 < RY ? rows - row0 : RY);
+      const int total = nr * segs;
+      const int first = (warp - offset + kConsumerWarps) % kConsumerWarps;  // this warp's first segment
+      offset = (offset + total) % kConsumerWarps;
+      if (first >= total) {  // no segment of this item for this warp
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
         if (++s == S_) { s = 0; ph ^= 1u; }
@@ -222,37 +229,32 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
       const float corrf = (float)corr;
       const float corrf_s = corrf * F16S_INV_SCALE;
       const float tau0f = (float)ia.tau0, ksmagf = (float)ia.k_smag;
-      int iy = 0, iz = 0;
-      if (row_ok) {
-        const int2 yz = s_row[s * kMaxRowsPerItem + ry];
-        iy = yz.x;
-        iz = yz.y;
-      }
-      const T* sp = spop + (size_t)s * b.slot_elems + (size_t)ry * 19 * pitch;
-      const uint8_t* sc = scls + (size_t)s * b.slot_cls + (size_t)ry * pitch;
-      const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
-      const int seg = (warp % wpr + j) % wpr;
-      const int nchunks = (nx + shift + span - 1) / span;
       T* fd = static_cast<T*>(b.bufs[2 * k + (cur ^ 1)]);
       long long item_sum = 0;
       int my_nan = 0;
-      for (int c = 0; c < nchunks; ++c) {
-        const int cell_lo = c * span + seg * 32 - shift;
+      for (int sg = first; sg < total; sg += kConsumerWarps) {
+        const int ry = sg / segs;
+        const int cell_lo = (sg - ry * segs) * 32 - shift;
+        const int2 yz = s_row[s * kMaxRowsPerItem + ry];
+        const int iy = yz.x, iz = yz.y;
+        const T* sp = spop + (size_t)s * b.slot_elems + (size_t)ry * 19 * pitch;
+        const uint8_t* sc = scls + (size_t)s * b.slot_cls + (size_t)ry * pitch;
         const int ix = cell_lo + lane;
-        const bool active = row_ok && ix >= 0 && ix < nx;
-        const int lx = (ix >= 0 && ix < nx) ? ix : 1;
+        const bool active = ix >= 0 && ix < nx;
+        const int lx = active ? ix : 1;
         const uint8_t cl = sc[lx];
         float v[19];
 #pragma unroll
         for (int d = 0; d < 19; ++d) v[d] = S::h_scaled(sp[slot_of(d) * pitch + lx - cx_of(d)], d, corrf, corrf_s);
-        if (c == nchunks - 1) {
+        if (sg + kConsumerWarps >= total) {  // this warp's last segment of the slot
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);
         }
         SegGeom g;
-        g.row = row; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
+        g.row = row0 + ry; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
         g.iy = iy; g.iz = iz; g.cell_lo = cell_lo; g.ix = ix; g.flag = cl & CLS_FLAG_MASK;
-        g.row_ok = row_ok; g.active = active; g.near = (cl & CLS_NEAR) != 0; g.wall_row = wall_row;
+        g.row_ok = true; g.active = active; g.near = (cl & CLS_NEAR) != 0;
+        g.wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
         g.ground_no_slip = ia.ground_no_slip; g.write_macro = b.write_macro; g.cl = cl;
         fast_segment<S>(v, fd, g, tau0f, ksmagf,
                         [&](int y) {

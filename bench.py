@@ -223,6 +223,10 @@ def run_ours(args) -> dict:
                                   "frac": round(ach2 / hbm, 4), "traffic": _profile_traffic(prec)}}
         e2.close()
 
+    # ---- batched sweep: 32 wings of uneven lattice sizes, one launch per step ----
+    if args.batch_steps > 0:
+        out["batch"] = run_batch(args, dev, ws, barrier_sync, max_over_ranks)
+
     # ---- Cd / Cl / Cm error of reduced storage vs the FP64 GPU run.  The flow at
     # Re = 2e4 is unsteady and chaotic, so runs that differ only in rounding drift
     # apart sample by sample: the coefficients are compared as time averages over
@@ -271,6 +275,63 @@ def run_ours(args) -> dict:
                    "parallelism": f"{ws} independent lattices, one per GPU (weak scaling)"},
     })
     return out if rank == 0 else {}
+
+
+def run_batch(args, dev: int, ws: int, barrier_sync, max_over_ranks) -> dict:
+    """The batched angle-of-attack sweep (32 extruded NACA 0012 wings, lattices
+    128x64x64 .. 190x95x95, FP16 shifted storage) in one persistent launch per step:
+    autotuned launch configuration, device-timed steps, per-instance Cd / Cl averaged
+    over the last fifth of the run (a force sample every 200 steps)."""
+    from aerosim_b200 import LBMBatch
+    from aerosim_b200 import cases
+    cs = cases.naca_batch(steps=args.batch_steps)
+    engines, vox_ms = [], 0.0
+    for c in cs:
+        e, info = _make_engine(c, "f16s", dev)
+        engines.append(e)
+        vox_ms += info.voxelization_time_ms
+    b = LBMBatch(engines)
+    tune = b.autotune(20)
+    b.step(args.warmup)
+    barrier_sync()
+    window = max(1, args.batch_steps // 5)
+    every = min(200, window)
+    total_ms, launches = 0.0, 0
+    b.step(args.batch_steps - window)
+    ms, n = b.last_step_timing()
+    total_ms += ms
+    launches += n
+    cd, cl, samples, left = np.zeros(len(cs)), np.zeros(len(cs)), 0, window
+    while left > 0:
+        k = min(every, left)
+        b.step(k)
+        ms, n = b.last_step_timing()
+        total_ms += ms
+        launches += n
+        for i, e in enumerate(engines):
+            f = e.read_forces()
+            cd[i] += f.cd
+            cl[i] += f.cl
+        samples += 1
+        left -= k
+    barrier_sync()
+    total_ms = max_over_ranks(total_ms)
+    nan = any(e.mass_stats()["hasNaN"] for e in engines)
+    cells = b.cells
+    b.close()
+    for e in engines:
+        e.close()
+    return {"workload": f"naca0012_x{len(cs)}_128x64x64..190x95x95_f16s", "instances": len(cs),
+            "cells_per_gpu": cells, "steps": args.batch_steps,
+            "mlups": round(ws * cells * args.batch_steps / (total_ms * 1e-3) / 1e6, 1),
+            "ms_per_step": total_ms / args.batch_steps, "gpu_launches": int(launches),
+            "tuning": tune, "voxelization_ms_total": round(vox_ms, 1),
+            "aoa_deg": [round(c.extra["aoa_deg"], 2) for c in cs],
+            "cd_mean": [round(float(v / samples), 4) for v in cd],
+            "cl_mean": [round(float(v / samples), 4) for v in cl],
+            "force_window": f"last {window} steps, every {every}", "nan": nan,
+            "note": "one persistent launch per batched step over the rows of all 32 lattices; "
+                    "runs of steps replayed from a CUDA graph; device-timed"}
 
 
 def cpu_sample(case, threads: int, seconds: float, steps_cap: int | None = None) -> dict:
@@ -335,6 +396,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cd-steps", type=int, default=20000, help="steps of the FP64-oracle Cd comparison (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--batch-steps", type=int, default=10000,
+                    help="steps of the batched 32-wing sweep (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI frame loop")
     ap.add_argument("--precisions", default="f32,f16s,bf16s",
