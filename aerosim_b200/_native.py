@@ -109,6 +109,15 @@ SIGNATURES = {
     "aerosim_batch_get_tuning": ([_P, C.POINTER(BatchTuning)], C.c_int),
     "aerosim_batch_last_timing": ([_P, _F64P, C.POINTER(C.c_int64)], C.c_int),
     "aerosim_batch_cells": ([_P, C.POINTER(C.c_int64)], C.c_int),
+    "aerosim_mlp_param_count": ([], C.c_int),
+    "aerosim_mlp_forward": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
+    "aerosim_mlp_forward_tc": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
+    "aerosim_mlp_gradients": ([_F32P, _F32P, _F32P, C.c_int64, _F32P, _F64P], C.c_int),
+    "aerosim_mlp_train": ([_F32P, _F32P, _F32P, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _F32P],
+                          C.c_int),
+    "aerosim_set_sgs_mlp": ([_P, _F32P], C.c_int),
+    "aerosim_read_wall_distance": ([_P, _F32P], C.c_int),
+    "aerosim_sgs_samples": ([_P, _P, C.c_float, _F32P, _F32P, _U8P], C.c_int),
     "aerosim_frontal_area": ([_F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P], C.c_int),
     "aerosim_momentum_exchange_noalloc": ([_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, C.c_int32, _P, _P],
                                           C.c_int),

@@ -9,6 +9,7 @@ Translation units and their floating-point contracts:
   voxelize.cu   FP64 BVH voxelizer, bit-exact flags and links: -fmad=false
   engine.cu     C-ABI host layer
   noalloc.cu    allocation-free force reduction entry point: -fmad=false
+  sgs.cu        learned SGS closure: MLP training, wall distance, training samples
 """
 from __future__ import annotations
 
@@ -38,6 +39,7 @@ UNITS = {
     "voxelize.cu": ["-fmad=false"],
     "engine.cu": [],
     "noalloc.cu": ["-fmad=false"],
+    "sgs.cu": [],
 }
 
 

@@ -15,6 +15,7 @@
 #include "engine_internal.h"
 #include "lbm_kernels.cuh"
 #include "lbm_batch.cuh"
+#include "sgs_mlp.cuh"
 
 using namespace aerosim;
 
@@ -58,6 +59,10 @@ struct aerosim_engine {
   long long step_index = 0;
   double last_ms = 0;
   long long last_launches = 0;
+  // learned SGS closure (null: Smagorinsky)
+  uint32_t* mlp_frag = nullptr;
+  float* mlp_bias = nullptr;
+  bool wall_ready = false;  // wall distances in the class bytes
 };
 
 namespace {
@@ -129,13 +134,15 @@ int configure_step(aerosim_engine* h) {
   const size_t eb = precision_bytes(h->cfg.precision);
   const dim3 block(kStepThreads, 1, 1);
   StepArgs dummy{};
-  dummy.L = L;  // the kernel instance depends on the row pitch
+  dummy.L = L;  // the kernel instance depends on the row pitch and the closure
+  dummy.mlp_frag = h->mlp_frag;
+  const bool mlp = h->mlp_frag != nullptr;
   const char* env = getenv("AEROSIM_STAGES");
   const int forced = env ? atoi(env) : 0;
   int best_s = 0, best_occ = 0;
   for (int S = 2; S <= 8; ++S) {
     if (forced && S != forced) continue;
-    const size_t smem = step_smem_bytes(L, S, eb);
+    const size_t smem = step_smem_bytes(L, S, eb, mlp);
     if (smem > 227 * 1024) break;
     int occ = 0;
     cudaError_t e = launch_step(h->cfg.precision, dummy, block, 0, smem, h->stream, &occ, nullptr);
@@ -149,7 +156,7 @@ int configure_step(aerosim_engine* h) {
   if (best_s == 0) return fail(h, AEROSIM_ERR_ARG, "step kernel: no launch configuration fits shared memory");
   h->block = block;
   h->stages = best_s;
-  h->smem = step_smem_bytes(L, best_s, eb);
+  h->smem = step_smem_bytes(L, best_s, eb, mlp);
   // the occupancy of the chosen configuration
   CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ, nullptr));
   h->occupancy = best_occ;
@@ -304,6 +311,11 @@ int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[
     if (nn) CU(h, cudaMemcpy(h->near_cells, nearv.data(), nn * 4, cudaMemcpyHostToDevice));
     CU(h, cudaMemcpy(h->links, links.data(), links.size() * sizeof(NearLink), cudaMemcpyHostToDevice));
   }
+  h->wall_ready = false;
+  if (h->mlp_frag) {  // the learned closure reads wall distances from the class bytes
+    CU(h, compute_wall_distance(ng.flags, ng.nx, ng.ny, ng.nz, nullptr, ng.cls, nl.pitch, h->stream));
+    h->wall_ready = true;
+  }
   if (h->f[0] && (nl.pitch != h->L.pitch || nl.plane != h->L.plane)) free_pops(h);
   free_grid(h->g);
   h->g = ng;
@@ -417,6 +429,7 @@ int aerosim_destroy(aerosim_engine* h) {
   cudaFree(h->near_cells); cudaFree(h->links);
   cudaFree(h->force_partials); cudaFree(h->force_ticket); cudaFree(h->force_out);
   cudaFree(h->stats_buf); cudaFree(h->staging);
+  cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -600,6 +613,9 @@ int aerosim_step(aerosim_engine* h, int32_t n) {
   a.tau0 = 3.0 * h->cfg.nu_lattice + 0.5;
   const double cs2 = h->cfg.smagorinsky_cs * h->cfg.smagorinsky_cs;
   a.k_smag = 18.0 * M_SQRT2 * cs2;
+  a.mlp_frag = h->mlp_frag;
+  a.mlp_bias = h->mlp_bias;
+  a.mlp_nu0 = (float)((std::max(a.tau0, 0.5015) - 0.5) / 3.0);
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < n; ++s) {
@@ -813,6 +829,105 @@ int aerosim_frontal_area(const float* pos, int64_t nv, const int32_t* idx, int64
   long long covered = 0;
   for (uint16_t c : cover) covered += __builtin_popcount(c);
   *out = ((double)covered / ((double)res * res * 16)) * (span_y * span_z);
+  return AEROSIM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Learned SGS closure of an engine.
+// ---------------------------------------------------------------------------
+namespace {
+
+int ensure_wall_distance(aerosim_engine* h) {
+  if (h->wall_ready) return AEROSIM_OK;
+  CU(h, compute_wall_distance(h->g.flags, h->g.nx, h->g.ny, h->g.nz, nullptr, h->g.cls, h->L.pitch, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  h->wall_ready = true;
+  return AEROSIM_OK;
+}
+
+double effective_nu0(const aerosim_engine* h) {
+  return (std::max(3.0 * h->cfg.nu_lattice + 0.5, 0.5015) - 0.5) / 3.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aerosim_set_sgs_mlp(aerosim_engine* h, const float* params) {
+  if (!h) return AEROSIM_ERR_ARG;
+  CU(h, cudaSetDevice(h->device));
+  if (!params) {
+    cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
+    h->mlp_frag = nullptr;
+    h->mlp_bias = nullptr;
+  } else {
+    for (int i = 0; i < kMlpParams; ++i)
+      if (!std::isfinite(params[i])) return fail(h, AEROSIM_ERR_ARG, "set_sgs_mlp: non-finite parameter");
+    std::vector<uint32_t> frag(kMlpFragWords * 32);
+    std::vector<float> bias(kMlpBias);
+    mlp_pack_fragments(params, frag.data(), bias.data());
+    if (!h->mlp_frag) {
+      CU(h, cudaMalloc(&h->mlp_frag, frag.size() * sizeof(uint32_t)));
+      CU(h, cudaMalloc(&h->mlp_bias, bias.size() * sizeof(float)));
+    }
+    CU(h, cudaMemcpy(h->mlp_frag, frag.data(), frag.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CU(h, cudaMemcpy(h->mlp_bias, bias.data(), bias.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (h->have_grid) {
+      int rc = ensure_wall_distance(h);
+      if (rc) return rc;
+    }
+  }
+  if (h->have_grid && h->f[0]) return configure_step(h);
+  return AEROSIM_OK;
+}
+
+int aerosim_read_wall_distance(aerosim_engine* h, float* out) {
+  if (!h || !out) return AEROSIM_ERR_ARG;
+  if (!h->have_grid) return fail(h, AEROSIM_ERR_STATE, "read_wall_distance: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  const long long N = h->g.N;
+  int rc = ensure_staging(h, N * sizeof(float));
+  if (rc) return rc;
+  CU(h, compute_wall_distance(h->g.flags, h->g.nx, h->g.ny, h->g.nz, static_cast<float*>(h->staging), h->g.cls,
+                              h->L.pitch, h->stream));
+  h->wall_ready = true;
+  CU(h, cudaMemcpyAsync(out, h->staging, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
+int aerosim_sgs_samples(aerosim_engine* fine, aerosim_engine* coarse, float max_ratio, float* X, float* Y,
+                        uint8_t* valid) {
+  if (!fine || !coarse || !X || !Y || !valid || !(max_ratio > 0.0f))
+    return fail(nullptr, AEROSIM_ERR_ARG, "sgs_samples: bad argument");
+  if (!fine->have_grid || !fine->f[0] || !coarse->have_grid)
+    return fail(nullptr, AEROSIM_ERR_STATE, "sgs_samples: both engines need a voxel grid (and the fine one a flow)");
+  if (fine->device != coarse->device) return fail(nullptr, AEROSIM_ERR_ARG, "sgs_samples: engines on different devices");
+  const DevGrid &f = fine->g, &c = coarse->g;
+  if (f.nx != 2 * c.nx || f.ny != 2 * c.ny || f.nz != 2 * c.nz)
+    return fail(nullptr, AEROSIM_ERR_ARG, "sgs_samples: the fine lattice must be exactly twice the coarse one");
+  CU(coarse, cudaSetDevice(coarse->device));
+  CU(fine, cudaStreamSynchronize(fine->stream));
+  int rc = ensure_wall_distance(coarse);
+  if (rc) return rc;
+  const long long Nc = c.N;
+  float *dx = nullptr, *dy = nullptr;
+  uint8_t* dv = nullptr;
+  cudaError_t e = cudaMalloc(&dx, Nc * kMlpIn * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dy, Nc * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dv, Nc);
+  if (e == cudaSuccess)
+    e = launch_sgs_samples(fine->mux, fine->muy, fine->muz, fine->mrho, f.flags, f.nx, f.ny, f.nz, c.cls,
+                           coarse->L.pitch, c.nx, c.ny, c.nz, (float)effective_nu0(coarse), max_ratio, dx, dy, dv,
+                           coarse->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(X, dx, Nc * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, coarse->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(Y, dy, Nc * sizeof(float), cudaMemcpyDeviceToHost, coarse->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(valid, dv, Nc, cudaMemcpyDeviceToHost, coarse->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(coarse->stream);
+  cudaFree(dx); cudaFree(dy); cudaFree(dv);
+  if (e != cudaSuccess) return fail(nullptr, AEROSIM_ERR_CUDA, std::string("sgs_samples: ") + cudaGetErrorString(e));
   return AEROSIM_OK;
 }
 

@@ -65,4 +65,14 @@ cudaError_t launch_mass_stats(const float* mux, const float* muy, const float* m
                               const uint8_t* cls, const StepState* st, int prev_slot, const Layout& L,
                               long long N, unsigned long long* out, cudaStream_t s);
 
+// sgs.cu: jump-flood wall distance of a dense flag array into float distances (dist,
+// may be null) and bits 3..7 of the pitched class bytes (cls, may be null); training
+// samples of the learned closure from a fine flow's macro fields and a 2x coarser grid.
+cudaError_t compute_wall_distance(const uint8_t* flags, int nx, int ny, int nz, float* dist, uint8_t* cls, int pitch,
+                                  cudaStream_t s);
+cudaError_t launch_sgs_samples(const float* ux, const float* uy, const float* uz, const float* rho,
+                               const uint8_t* fflags, int fx, int fy, int fz, const uint8_t* ccls, int cpitch, int cx,
+                               int cy, int cz, float nu0, float max_ratio, float* X, float* Y, uint8_t* valid,
+                               cudaStream_t s);
+
 }  // namespace aerosim

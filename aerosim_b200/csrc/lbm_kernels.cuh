@@ -19,6 +19,7 @@
 //     19 writes and one class byte per cell.
 #pragma once
 #include "common.cuh"
+#include "sgs_mlp.cuh"
 
 namespace aerosim {
 
@@ -28,9 +29,10 @@ enum { MODE_FAST = 0, MODE_MIRROR = 1, MODE_F64 = 2 };
 // from a third CTA (more warps in flight per SM: 131 -> 121 us per step measured at
 // 256x128x128, with some spilling at 64 registers); the 16-bit storage kernels issue
 // more instructions per cell and lose more to spills at that budget, so they keep two.
-template <class S, int MODE>
+// With the learned closure the tensor-core MLP needs registers: two CTAs.
+template <class S, int MODE, bool MLP = false>
 constexpr int step_min_blocks() {
-  return MODE != MODE_FAST ? 1 : (sizeof(typename S::T) == 4 ? 3 : 2);
+  return MODE != MODE_FAST ? 1 : (MLP ? 2 : (sizeof(typename S::T) == 4 ? 3 : 2));
 }
 
 struct NearLink;
@@ -58,6 +60,11 @@ struct StepArgs {
   int write_macro;
   int ground_no_slip;
   double u_inlet, tau0, k_smag;  // k_smag = 18 * SQRT2 * Cs^2
+  // learned SGS closure (null: Smagorinsky): packed BF16 weight fragments and biases
+  // (sgs_mlp.cuh) and the molecular viscosity nu_0 its output is scaled by
+  const uint32_t* mlp_frag;
+  const float* mlp_bias;
+  float mlp_nu0;
 };
 
 struct ForceArgs {
@@ -286,9 +293,21 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 // from (lbmCpuReference.ts:233-262), j = rho u.  The results are written back into
 // h[] already in the storage domain of S (kOutScale * h + kOutW * w), the storage's
 // scale and rest weight folded into the per-direction constants.
-template <class S>
+// With MLP the eddy viscosity comes from the learned closure (sgs_mlp.cuh) evaluated
+// by the whole warp on the tensor cores: tau = 3 nu_0 (1 + nu_t / nu_0) + 1/2, with the
+// Smagorinsky tau as the fallback when the network returns a non-finite value.
+struct MlpRefs {
+  const uint32_t* frag;  // shared memory
+  const float* bias;
+  uint32_t* stage;       // the warp's 32 x 8 BF16 staging block
+  float nu0;
+  float wall_dist;       // this lane's cell
+  int lane;
+};
+
+template <class S, bool MLP = false>
 __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux, float& uy, float& uz,
-                                             float tau0, float k_smag) {
+                                             float tau0, float k_smag, const MlpRefs* m = nullptr) {
   constexpr float OS = S::kOutScale, OW = S::kOutW;
   constexpr float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
   float s[9], t[9];
@@ -323,7 +342,14 @@ __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux
   const float pxy = fmaf(-jcx, uy, sxy), pxz = fmaf(-jcx, uz, sxz), pyz = fmaf(-jcy, uz, syz);
   const float off = fmaf(pxy, pxy, fmaf(pxz, pxz, pyz * pyz));
   const float pn = sqrt_approx(fmaf(pxx, pxx, fmaf(pyy, pyy, fmaf(pzz, pzz, 2.0f * off))));
-  const float tau = 0.5f * (tau0 + sqrt_approx(fmaf(tau0, tau0, k_smag * pn * ir)));
+  float tau = 0.5f * (tau0 + sqrt_approx(fmaf(tau0, tau0, k_smag * pn * ir)));
+  if constexpr (MLP) {
+    float x[kMlpIn];
+    mlp_features(pxx, pyy, pzz, pxy, pxz, pyz, r, tau, m->wall_dist, x);
+    const float ratio = mlp_nut_warp(x, m->frag, m->bias, m->stage, m->lane);
+    const float tm = fmaf(3.0f * m->nu0, 1.0f + ratio, 0.5f);
+    if (tm == tm && tm < 1.0e30f) tau = tm;
+  }
   const float om = rcp_approx(fmaxf(0.5015f, fminf(1.95f, tau)));
   const float xxx = fmaf(-om, pxx, dxx), xyy = fmaf(-om, pyy, dyy), xzz = fmaf(-om, pzz, dzz);
   const float xxy = fmaf(-om, pxy, sxy), xxz = fmaf(-om, pxz, sxz), xyz = fmaf(-om, pyz, syz);
@@ -437,10 +463,12 @@ __host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem)
   return (size_t)rows_per_item(L.nx) * (19 * (size_t)L.pitch * elem + (size_t)L.pitch);
 }
 constexpr size_t kSmemGuard = 64;
-__host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem) {
+// With the learned closure: its weight fragments, biases and per-warp staging blocks.
+__host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem, bool mlp = false) {
   return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 + 16 * (size_t)stages +
          2 * (size_t)L.ny * sizeof(double) + (size_t)stages * rows_per_item(L.nx) * sizeof(int2) +
-         kConsumerWarps * 20 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int);
+         kConsumerWarps * 20 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int) +
+         (mlp ? (kMlpFragWords * 32 + kMlpBias + 3 + kConsumerWarps * 128) * 4 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -737,18 +765,24 @@ struct SegGeom {
   uint8_t cl;               // this lane's class byte
 };
 
-template <class S, class InletFn>
+template <class S, class InletFn, bool MLP = false>
 __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __restrict__ fd, const SegGeom g,
                                              float tau0, float k_smag, InletFn inlet_u, const StepArgs& m,
                                              float* xo, const float4* s_dcw, const int* s_dslot, int lane,
-                                             long long& my_sum, int& my_nan) {
+                                             long long& my_sum, int& my_nan, const MlpRefs* mlp = nullptr) {
   using T = typename S::T;
   const int nx = g.nx, ny = g.ny, nz = g.nz, pitch = g.pitch, cell_lo = g.cell_lo, ix = g.ix;
   const long long row = g.row;
   T* const blk = fd + row * 19 * pitch;
   const bool own = g.active && g.flag != CELL_SOLID && !g.near && ix != 0 && ix != nx - 1;
   float r, ux, uy, uz;
-  collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag);  // v: storage domain
+  if constexpr (MLP) {
+    MlpRefs mr = *mlp;
+    mr.wall_dist = (float)(g.cl >> 3);
+    collide_fast<S, true>(v, r, ux, uy, uz, tau0, k_smag, &mr);  // v: storage domain
+  } else {
+    collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag);
+  }
   if (g.row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
     // inlet (:328-352): density of ix = 1 (1 for a solid, :177); a near-wall ix = 1
     // defers the inlet to the near-wall pass, a solid ix = 0 has none
@@ -838,8 +872,8 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
   }
 }
 
-template <class S, int MODE, int P>
-__global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE>())
+template <class S, int MODE, int P, bool MLP = false>
+__global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     main_kernel(const __grid_constant__ StepArgs a) {
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
@@ -872,6 +906,14 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE>())
   float4* s_dcw = reinterpret_cast<float4*>(
       (reinterpret_cast<uintptr_t>(s_xo + kConsumerWarps * 20) + 15) & ~uintptr_t(15));  // [19]
   int* s_dslot = reinterpret_cast<int*>(s_dcw + 19);                                     // [19]
+  // learned closure: weight fragments, biases, one staging block per consumer warp
+  uint32_t* s_mfrag = reinterpret_cast<uint32_t*>(s_dslot + 19);                          // [24 * 32]
+  float* s_mbias = reinterpret_cast<float*>(s_mfrag + kMlpFragWords * 32);               // [65]
+  uint32_t* s_mstage = reinterpret_cast<uint32_t*>(s_mbias + kMlpBias + 3);              // [8][128]
+  if constexpr (MLP) {
+    for (int i = threadIdx.x; i < kMlpFragWords * 32; i += blockDim.x) s_mfrag[i] = a.mlp_frag[i];
+    for (int i = threadIdx.x; i < kMlpBias; i += blockDim.x) s_mbias[i] = a.mlp_bias[i];
+  }
 
   const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
   T* __restrict__ fd = static_cast<T*>(a.fdst);
@@ -1043,9 +1085,15 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE>())
           g.iy = iy; g.iz = iz; g.cell_lo = cell_lo; g.ix = ix; g.flag = flag;
           g.row_ok = row_ok; g.active = active; g.near = near; g.wall_row = wall_row;
           g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro; g.cl = cl;
-          fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag,
-                          [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); }, a,
-                          s_xo + warp * 20, s_dcw, s_dslot, lane, my_sum, my_nan);
+          auto inlet = [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); };
+          if constexpr (MLP) {
+            const MlpRefs mr{s_mfrag, s_mbias, s_mstage + warp * 128, a.mlp_nu0, 0.0f, lane};
+            fast_segment<S, decltype(inlet), true>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a,
+                                                   s_xo + warp * 20, s_dcw, s_dslot, lane, my_sum, my_nan, &mr);
+          } else {
+            fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a, s_xo + warp * 20, s_dcw, s_dslot,
+                            lane, my_sum, my_nan);
+          }
         } else {
           CellCtx cc;
           cc.row = row; cc.ix = ix; cc.iy = iy; cc.iz = iz; cc.cell_lo = cell_lo; cc.flag = flag;

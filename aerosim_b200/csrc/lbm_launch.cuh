@@ -25,10 +25,10 @@ cudaError_t raise_smem_limit(K k) {
 
 // One time step: a single main_kernel launch.  Returns the number of launches in
 // *launches.
-template <class S, int MODE, int P>
+template <class S, int MODE, int P, bool MLP = false>
 cudaError_t step_entry(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s, int* occ,
                        int* launches) {
-  auto k = main_kernel<S, MODE, P>;
+  auto k = main_kernel<S, MODE, P, MLP>;
   if (occ) {
     cudaError_t e = raise_smem_limit(k);
     if (e != cudaSuccess) return e;
@@ -41,11 +41,19 @@ cudaError_t step_entry(const StepArgs& a, dim3 block, unsigned grid, size_t smem
 
 // The FP32-arithmetic kernels are compiled for every row pitch up to 256 (multiples
 // of 32) with the pitch as a constant; other pitches and the double modes take the
-// run-time pitch.
+// run-time pitch.  With the learned closure (a.mlp_frag set): pitches 128 and 256, or
+// the run-time pitch.
 template <class S, int MODE>
 cudaError_t step_dispatch(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s, int* occ,
                           int* launches) {
   if constexpr (MODE == MODE_FAST) {
+    if (a.mlp_frag) {
+      switch (a.L.pitch) {
+        case 128: return step_entry<S, MODE, 128, true>(a, block, grid, smem, s, occ, launches);
+        case 256: return step_entry<S, MODE, 256, true>(a, block, grid, smem, s, occ, launches);
+        default: return step_entry<S, MODE, 0, true>(a, block, grid, smem, s, occ, launches);
+      }
+    }
     switch (a.L.pitch) {
       case 32: return step_entry<S, MODE, 32>(a, block, grid, smem, s, occ, launches);
       case 64: return step_entry<S, MODE, 64>(a, block, grid, smem, s, occ, launches);

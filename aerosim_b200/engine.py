@@ -299,6 +299,26 @@ class LBMEngine:
             out["macroField"] = self.read_macro()
         return out
 
+    def set_sgs_mlp(self, params) -> None:
+        """Learned SGS closure (aerosim_b200.sgs parameters) for the following steps;
+        None restores Smagorinsky."""
+        if params is None:
+            self._h.call("aerosim_set_sgs_mlp", None)
+        else:
+            p = np.ascontiguousarray(params, dtype=np.float32)
+            self._h.call("aerosim_set_sgs_mlp", N.ptr(p, C.c_float))
+
+    def read_wall_distance(self) -> np.ndarray:
+        info = self.voxel_info()
+        out = np.empty(info.nx * info.ny * info.nz, np.float32)
+        self._h.call("aerosim_read_wall_distance", N.ptr(out, C.c_float))
+        return out
+
+    def voxel_info(self) -> N.VoxelInfo:
+        info = N.VoxelInfo()
+        self._h.call("aerosim_get_voxel_info", C.byref(info))
+        return info
+
     def close(self) -> None:
         self._h.close()
 

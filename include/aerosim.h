@@ -189,6 +189,40 @@ int aerosim_momentum_exchange_noalloc(const float* f, const uint8_t* flags, cons
                                       const float* q, int64_t boundary_count, int32_t nx, int32_t ny,
                                       int32_t nz, double* out, void* stream);
 
+/* ---- learned subgrid-scale closure ----------------------------------------- */
+
+/* A per-cell MLP (8 inputs -> 32 -> 32 -> 1, GELU; inputs: the strain rate estimated
+ * from the non-equilibrium stress (6), density, wall distance) predicts nu_t / nu_0 in
+ * place of the Smagorinsky eddy viscosity.  No counterpart in the reference, whose
+ * closure is Smagorinsky only (src/solver/lbmCpuReference.ts:264-282); Smagorinsky
+ * stays the fallback.  Parameter layout (aerosim_mlp_param_count() floats): W1[32][8],
+ * b1[32], W2[32][32], b2[32], W3[32], b3.  The functions below take host arrays. */
+int aerosim_mlp_param_count(void);
+/* FP32 forward pass over n rows of X[n][8] (CUDA cores). */
+int aerosim_mlp_forward(const float* params, const float* X, int64_t n, float* out);
+/* The step kernel's evaluation: BF16 weights on the tensor cores, FP32 accumulation. */
+int aerosim_mlp_forward_tc(const float* params, const float* X, int64_t n, float* out);
+/* Mean squared error against Y[n] and its gradient with respect to the parameters. */
+int aerosim_mlp_gradients(const float* params, const float* X, const float* Y, int64_t n, float* grad,
+                          double* loss);
+/* Adam on the GPU: iters mini-batches of `batch` rows drawn by a seeded hash; params
+ * in/out; loss_curve[iters] (may be NULL) receives each mini-batch loss. */
+int aerosim_mlp_train(float* params, const float* X, const float* Y, int64_t n, int32_t iters, int32_t batch,
+                      float lr, uint64_t seed, float* loss_curve);
+/* params: the closure's weights for this engine's steps, NULL for Smagorinsky.  The
+ * F32, F16S and BF16S precisions use it (near-wall Bouzidi cells keep Smagorinsky). */
+int aerosim_set_sgs_mlp(aerosim_engine* h, const float* params);
+/* Euclidean distance (cells) of every cell centre to the nearest solid cell centre
+ * (jump flooding), float[nx*ny*nz]. */
+int aerosim_read_wall_distance(aerosim_engine* h, float* out);
+/* Training samples of the closure from the flow of `fine` (its macro fields of the last
+ * step) box-filtered onto `coarse`, whose lattice is exactly half as fine: per coarse
+ * cell X[8] (filtered strain rate, density, wall distance as the closure sees them),
+ * Y = nu_t / nu_0 of the least-squares eddy viscosity of the subgrid stress, capped at
+ * max_ratio, and valid (0 at solid, boundary-adjacent and edge cells). */
+int aerosim_sgs_samples(aerosim_engine* fine, aerosim_engine* coarse, float max_ratio, float* X, float* Y,
+                        uint8_t* valid);
+
 /* ---- batches: many tunnels in one launch --------------------------------- */
 
 /* A batch steps many wind-tunnel instances (angle-of-attack or specimen sweeps, uneven
