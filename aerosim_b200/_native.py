@@ -117,7 +117,7 @@ SIGNATURES = {
                           C.c_int),
     "aerosim_set_sgs_mlp": ([_P, _F32P], C.c_int),
     "aerosim_read_wall_distance": ([_P, _F32P], C.c_int),
-    "aerosim_sgs_samples": ([_P, _P, C.c_float, _F32P, _F32P, _U8P], C.c_int),
+    "aerosim_sgs_samples": ([_P, _P, C.c_float, C.c_int32, _F32P, _F32P, _U8P], C.c_int),
     "aerosim_frontal_area": ([_F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P], C.c_int),
     "aerosim_momentum_exchange_noalloc": ([_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, C.c_int32, _P, _P],
                                           C.c_int),

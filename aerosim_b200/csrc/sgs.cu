@@ -254,12 +254,12 @@ __global__ void sgs_filter_kernel(const float* __restrict__ ux, const float* __r
 }
 
 // Pass 2: filtered strain rate (central differences), subgrid stress
-// tau = (u u)~ - u~ u~ and the least-squares eddy viscosity nu_t = -tau_d : S / (2 S : S);
-// features as in mlp_features with the filtered strain rate, target nu_t / nu0.
+// tau = (u u)~ - u~ u~ and the two terms of the least-squares eddy viscosity
+// nu_t = -tau_d : S / (2 S : S): numerator and denominator per cell (0 where invalid);
+// features as in mlp_features with the filtered strain rate.
 __global__ void sgs_sample_kernel(const float* __restrict__ ubar, const float* __restrict__ uu,
-                                  const uint8_t* __restrict__ ccls, int cpitch, int cx, int cy, int cz, float nu0,
-                                  float max_ratio, float* __restrict__ Xo, float* __restrict__ Yo,
-                                  uint8_t* __restrict__ valid) {
+                                  const uint8_t* __restrict__ ccls, int cpitch, int cx, int cy, int cz,
+                                  float* __restrict__ Xo, float2* __restrict__ nd, uint8_t* __restrict__ valid) {
   const long long Nc = (long long)cx * cy * cz;
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < Nc; c += (long long)gridDim.x * blockDim.x) {
     const int X = (int)(c % cx);
@@ -274,7 +274,10 @@ __global__ void sgs_sample_kernel(const float* __restrict__ ubar, const float* _
       for (int a = 0; a < 3; ++a) g[a][bdir] = 0.5f * (ubar[p * 4 + a] - ubar[m * 4 + a]);
     }
     valid[c] = ok ? 1 : 0;
-    if (!ok) continue;
+    if (!ok) {
+      nd[c] = make_float2(0.0f, 0.0f);
+      continue;
+    }
     const float sxx = g[0][0], syy = g[1][1], szz = g[2][2];
     const float sxy = 0.5f * (g[0][1] + g[1][0]), sxz = 0.5f * (g[0][2] + g[2][0]), syz = 0.5f * (g[1][2] + g[2][1]);
     const float ux = ubar[c * 4], uy = ubar[c * 4 + 1], uz = ubar[c * 4 + 2], r = ubar[c * 4 + 3];
@@ -284,14 +287,43 @@ __global__ void sgs_sample_kernel(const float* __restrict__ ubar, const float* _
     t[0] -= tr; t[1] -= tr; t[2] -= tr;
     const float ss = sxx * sxx + syy * syy + szz * szz + 2.0f * (sxy * sxy + sxz * sxz + syz * syz);
     const float ts = t[0] * sxx + t[1] * syy + t[2] * szz + 2.0f * (t[3] * sxy + t[4] * sxz + t[5] * syz);
-    float nut = ss > 0.0f ? -ts / (2.0f * ss) : 0.0f;
-    nut = fminf(fmaxf(nut, 0.0f), max_ratio * nu0);
+    nd[c] = make_float2(-ts, 2.0f * ss);
     const float wd = (float)(ccls[R * cpitch + X] >> 3);
     float* xo = Xo + c * kMlpIn;
     xo[0] = 100.0f * sxx; xo[1] = 100.0f * syy; xo[2] = 100.0f * szz;
     xo[3] = 100.0f * sxy; xo[4] = 100.0f * sxz; xo[5] = 100.0f * syz;
     xo[6] = 100.0f * (r - 1.0f);
     xo[7] = wd * (1.0f / 16.0f);
+  }
+}
+
+// Pass 3: the target nu_t / nu_0 of a valid cell: numerators and denominators summed
+// over the valid cells of its (2 avg + 1)^3 neighbourhood, then divided and clipped to
+// [0, max_ratio] (least-squares averaging, which keeps the sign information that a
+// per-cell clip at zero would discard).
+__global__ void sgs_target_kernel(const float2* __restrict__ nd, const uint8_t* __restrict__ valid, int cx, int cy,
+                                  int cz, int avg, float nu0, float max_ratio, float* __restrict__ Yo) {
+  const long long Nc = (long long)cx * cy * cz;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < Nc; c += (long long)gridDim.x * blockDim.x) {
+    if (!valid[c]) {
+      Yo[c] = 0.0f;
+      continue;
+    }
+    const int X = (int)(c % cx);
+    const long long R = c / cx;
+    const int Y = (int)(R % cy), Z = (int)(R / cy);
+    float n = 0.0f, d = 0.0f;
+    for (int dz = -avg; dz <= avg; ++dz)
+      for (int dy = -avg; dy <= avg; ++dy)
+        for (int dx = -avg; dx <= avg; ++dx) {
+          const int xx = X + dx, yy = Y + dy, zz = Z + dz;
+          if (xx < 0 || yy < 0 || zz < 0 || xx >= cx || yy >= cy || zz >= cz) continue;
+          const float2 v = nd[xx + (long long)cx * (yy + (long long)cy * zz)];
+          n += v.x;
+          d += v.y;
+        }
+    float nut = d > 0.0f ? n / d : 0.0f;
+    nut = fminf(fmaxf(nut, 0.0f), max_ratio * nu0);
     Yo[c] = nut / nu0;
   }
 }
@@ -348,20 +380,24 @@ cudaError_t compute_wall_distance(const uint8_t* flags, int nx, int ny, int nz, 
 
 cudaError_t launch_sgs_samples(const float* ux, const float* uy, const float* uz, const float* rho,
                                const uint8_t* fflags, int fx, int fy, int fz, const uint8_t* ccls, int cpitch, int cx,
-                               int cy, int cz, float nu0, float max_ratio, float* X, float* Y, uint8_t* valid,
-                               cudaStream_t s) {
+                               int cy, int cz, float nu0, float max_ratio, int avg, float* X, float* Y,
+                               uint8_t* valid, cudaStream_t s) {
   const long long Nc = (long long)cx * cy * cz;
   float *ubar = nullptr, *uu = nullptr;
+  float2* nd = nullptr;
   cudaError_t e = cudaMallocAsync(&ubar, Nc * 4 * sizeof(float), s);
   if (e == cudaSuccess) e = cudaMallocAsync(&uu, Nc * 6 * sizeof(float), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&nd, Nc * sizeof(float2), s);
   const int grid = (int)std::min<long long>((Nc + 255) / 256, 148 * 16);
   if (e == cudaSuccess) {
     sgs_filter_kernel<<<grid, 256, 0, s>>>(ux, uy, uz, rho, fflags, fx, fy, fz, cx, cy, cz, ubar, uu);
-    sgs_sample_kernel<<<grid, 256, 0, s>>>(ubar, uu, ccls, cpitch, cx, cy, cz, nu0, max_ratio, X, Y, valid);
+    sgs_sample_kernel<<<grid, 256, 0, s>>>(ubar, uu, ccls, cpitch, cx, cy, cz, X, nd, valid);
+    sgs_target_kernel<<<grid, 256, 0, s>>>(nd, valid, cx, cy, cz, avg, nu0, max_ratio, Y);
     e = cudaGetLastError();
   }
   cudaFreeAsync(ubar, s);
   cudaFreeAsync(uu, s);
+  cudaFreeAsync(nd, s);
   return e;
 }
 
