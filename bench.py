@@ -41,10 +41,8 @@ WORKLOAD = "ellipsoid_256x128x128"
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from aerosim_b200 import distributed
+    return distributed.env()
 
 
 def _peaks():
@@ -139,11 +137,11 @@ def run_ours(args) -> dict:
     import torch
     from aerosim_b200 import _native as N
     from aerosim_b200 import cases
+    from aerosim_b200 import distributed
     ws, rank, local = _dist()
     if ws > 1:
-        import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        distributed.init("nccl", timeout_s=300)
     dev = local
     case = cases.ellipsoid_256x128x128(args.steps)
     cells = case.cells
@@ -151,17 +149,11 @@ def run_ours(args) -> dict:
     def barrier_sync():
         torch.cuda.synchronize(dev)
         if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+            distributed.barrier(f"cuda:{dev}")
             torch.cuda.synchronize(dev)
 
     def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return distributed.max_over_ranks(x, device=f"cuda:{dev}")
 
     out = {}
     # ---- headline: FP32, device-timed ----
