@@ -325,7 +325,8 @@ int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[
   h->dx = dx;
   h->origin[0] = origin[0]; h->origin[1] = origin[1]; h->origin[2] = origin[2];
   h->fluid_count = h->g.N - h->g.solid;
-  const long long blocks = std::max<long long>(1, (h->g.B + 255) / 256);
+  // force reduction: 8 boundary cells per CTA and round, at most 8 CTAs per SM
+  const long long blocks = std::max<long long>(1, std::min<long long>((h->g.B + 7) / 8, 8LL * h->num_sms));
   if (blocks > h->force_blocks_cap) {
     cudaFree(h->force_partials);
     h->force_partials = nullptr;
@@ -659,7 +660,7 @@ int aerosim_read_forces(aerosim_engine* h, aerosim_forces* out) {
     a.partials = h->force_partials; a.ticket = h->force_ticket; a.out = h->force_out;
     a.L = h->L; a.B = h->g.B;
     a.prev_slot = prev_slot(h);
-    const unsigned grid = (unsigned)((h->g.B + 255) / 256);
+    const unsigned grid = (unsigned)std::min<long long>((h->g.B + 7) / 8, h->force_blocks_cap);
     CU(h, launch_forces(h->cfg.precision, a, grid, h->stream));
     CU(h, cudaMemcpyAsync(r, h->force_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
     CU(h, cudaStreamSynchronize(h->stream));

@@ -1149,8 +1149,9 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
 
 // ---------------------------------------------------------------------------
 // Momentum exchange, forceIntegrator.ts:159-216, FP64 accumulation.
-// One thread per boundary cell; per-cell sums in the reference's link order, then a
-// deterministic tree across cells (warp shuffle -> CTA -> last CTA in block order).
+// One warp per boundary cell, lane l = link d = l + 1 (all 18 links' loads in flight
+// together), grid-stride over the cells; per-cell sums by a fixed shuffle tree, then
+// a deterministic tree across cells (warps -> CTA -> last CTA in block order).
 // ---------------------------------------------------------------------------
 template <class S, int MODE>
 __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
@@ -1158,7 +1159,7 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
   __shared__ double red[8][8];
   __shared__ bool is_last;
   const T* __restrict__ f = static_cast<const T*>(a.f);
-  const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int apply = a.prev_slot >= 0 ? a.st->apply[a.prev_slot] : 0;
   const double corr = apply ? a.st->corr[a.prev_slot] : 1.0;
   auto pop = [&](int d, long long i) -> double {
@@ -1166,25 +1167,32 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
     if constexpr (MODE == MODE_MIRROR) return (double)(float)(v * corr);
     else return v * corr;
   };
+  // this lane's link: direction d, its lattice vector and opposite
+  const int d = lane + 1;
+  int cx = 0, cy = 0, cz = 0, od = 0;
+  double w2 = 0.0;
+#pragma unroll
+  for (int e = 1; e < 19; ++e)
+    if (e == d) {
+      cx = cx_of(e); cy = cy_of(e); cz = cz_of(e); od = opp_of(e); w2 = 2.0 * w32_of(e);
+    }
+  const int nx = a.L.nx, ny = a.L.ny, nz = a.L.nz;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  if (b < a.B) {
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long b = (long long)blockIdx.x * (blockDim.x >> 5) + warp; b < a.B; b += warps) {
     const long long ci = a.bcells[b];
-    const int nx = a.L.nx, ny = a.L.ny, nz = a.L.nz;
     const int ix = (int)(ci % nx);
     const long long rem = (ci - ix) / nx;
     const int iy = (int)(rem % ny);
     const int iz = (int)((rem - iy) / ny);
-    double cfx = 0.0, cfy = 0.0, cfz = 0.0;
-    double cut = 0.0;
-#pragma unroll
-    for (int d = 1; d < 19; ++d) {
-      const double qv = (double)a.q[b * 18 + (d - 1)];
+    double cfx = 0.0, cfy = 0.0, cfz = 0.0, cut = 0.0;
+    if (lane < 18) {
+      const double qv = (double)a.q[b * 18 + lane];
       if (qv > 0.0) {
-        const int od = opp_of(d);
         const double fo = pop(d, ci);
-        const int ax = clampi(ix + cx_of(od), 0, nx - 1);
-        const int ay = clampi(iy + cy_of(od), 0, ny - 1);
-        const int az = clampi(iz + cz_of(od), 0, nz - 1);
+        const int ax = clampi(ix - cx, 0, nx - 1);  // cell + c_opp(d)
+        const int ay = clampi(iy - cy, 0, ny - 1);
+        const int az = clampi(iz - cz, 0, nz - 1);
         const long long ff = ax + (long long)nx * (ay + (long long)ny * az);
         double fi = fo;
         if ((a.cls[a.L.cls_at(ff)] & CLS_FLAG_MASK) != 1) {
@@ -1197,29 +1205,34 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
             fi = inv2q * fo + (1.0 - inv2q) * fic;
           }
         }
-        const double mom = fo + fi - 2.0 * w32_of(d);
-        cfx += (double)cx_of(d) * mom;
-        cfy += (double)cy_of(d) * mom;
-        cfz += (double)cz_of(d) * mom;
-        if (d <= 6) cut += 1.0;
+        const double mom = fo + fi - w2;
+        cfx = (double)cx * mom;
+        cfy = (double)cy * mom;
+        cfz = (double)cz * mom;
+        cut = d <= 6 ? 1.0 : 0.0;
       }
     }
-    const double rx = (ix + 0.5) - 0.5 * nx;
-    const double ry = (iy + 0.5) - 0.5 * ny;
-    const double rz = (iz + 0.5) - 0.5 * nz;
-    acc[0] = cfx; acc[1] = cfy; acc[2] = cfz;
-    acc[3] = ry * cfz - rz * cfy;
-    acc[4] = rz * cfx - rx * cfz;
-    acc[5] = rx * cfy - ry * cfx;
-    acc[6] = cut;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      cfx += __shfl_down_sync(0xffffffffu, cfx, o);
+      cfy += __shfl_down_sync(0xffffffffu, cfy, o);
+      cfz += __shfl_down_sync(0xffffffffu, cfz, o);
+      cut += __shfl_down_sync(0xffffffffu, cut, o);
+    }
+    if (lane == 0) {
+      const double rx = (ix + 0.5) - 0.5 * nx;
+      const double ry = (iy + 0.5) - 0.5 * ny;
+      const double rz = (iz + 0.5) - 0.5 * nz;
+      acc[0] += cfx; acc[1] += cfy; acc[2] += cfz;
+      acc[3] += ry * cfz - rz * cfy;
+      acc[4] += rz * cfx - rx * cfz;
+      acc[5] += rx * cfy - ry * cfx;
+      acc[6] += cut;
+    }
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < 7; ++k) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+  for (int k = 0; k < 7; ++k)
     if (lane == 0) red[warp][k] = acc[k];
-  }
   __syncthreads();
   if (threadIdx.x < 7) {
     double s = 0.0;
