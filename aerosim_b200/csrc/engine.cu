@@ -835,6 +835,32 @@ int aerosim_frontal_area(const float* pos, int64_t nv, const int32_t* idx, int64
 
 }  // extern "C"
 
+extern "C" int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fraction, int32_t mode, uint8_t* rgba,
+                                     int32_t* width, int32_t* height) {
+  if (!h || !width || !height) return AEROSIM_ERR_ARG;
+  if (axis < 0 || axis > 2 || mode < 0 || mode > 2) return fail(h, AEROSIM_ERR_ARG, "extract_slice: bad axis or mode");
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "extract_slice: no voxel grid");
+  const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz;
+  int w = nx, hh = ny;
+  if (axis == 1) { w = nx; hh = nz; }
+  else if (axis == 0) { w = nz; hh = ny; }
+  *width = w;
+  *height = hh;
+  if (!rgba) return AEROSIM_OK;
+  // the fixed coordinate, Math.min(n - 1, Math.max(0, Math.floor(fraction * n)))
+  const int n = axis == 0 ? nx : axis == 1 ? ny : nz;
+  const int fixed = (int)js_min(n - 1, js_max(0, std::floor(fraction * n)));
+  CU(h, cudaSetDevice(h->device));
+  const size_t bytes = (size_t)w * hh * 4;
+  int rc = ensure_staging(h, bytes);
+  if (rc) return rc;
+  CU(h, launch_slice(h->mux, h->muy, h->muz, h->mrho, h->g.cls, h->st, prev_slot(h), h->L, axis, fixed, mode,
+                     js_max(1e-4, h->cfg.u_inlet_lattice), w, hh, static_cast<uint8_t*>(h->staging), h->stream));
+  CU(h, cudaMemcpyAsync(rgba, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Learned SGS closure of an engine.
 // ---------------------------------------------------------------------------

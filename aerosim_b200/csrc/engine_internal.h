@@ -65,6 +65,11 @@ cudaError_t launch_mass_stats(const float* mux, const float* muy, const float* m
                               const uint8_t* cls, const StepState* st, int prev_slot, const Layout& L,
                               long long N, unsigned long long* out, cudaStream_t s);
 
+// Slice image of the macro fields (extractSliceRGBA): RGBA bytes [height][width].
+cudaError_t launch_slice(const float* mux, const float* muy, const float* muz, const float* mrho,
+                         const uint8_t* cls, const StepState* st, int prev_slot, const Layout& L, int axis, int fixed,
+                         int mode, double uref, int width, int height, uint8_t* rgba, cudaStream_t s);
+
 // sgs.cu: jump-flood wall distance of a dense flag array into float distances (dist,
 // may be null) and bits 3..7 of the pitched class bytes (cls, may be null); training
 // samples of the learned closure from a fine flow's macro fields and a 2x coarser grid.

@@ -177,4 +177,81 @@ __global__ void mass_stats_kernel(const float* __restrict__ mux, const float* __
   }
 }
 
+// ---- slice image: sampleCFDColormap + extractSliceRGBA, lbmCpuReference.ts:23-46, 499-596.
+// FP64 in the reference's operation order (this unit is built with -fmad=false), so the
+// bytes equal the reference's for the same macro fields.
+__device__ __forceinline__ void cfd_colormap(double tv, double (&rgb)[3]) {
+  const double t = js_max(0.0, js_min(1.0, tv));
+  if (t < 0.25) {
+    const double u = t * 4.0;
+    rgb[0] = 0.08 + (0.06 - 0.08) * u; rgb[1] = 0.22 + (0.72 - 0.22) * u; rgb[2] = 0.75 + (0.88 - 0.75) * u;
+  } else if (t < 0.5) {
+    const double u = (t - 0.25) * 4.0;
+    rgb[0] = 0.06 + (0.12 - 0.06) * u; rgb[1] = 0.72 + (0.82 - 0.72) * u; rgb[2] = 0.88 + (0.38 - 0.88) * u;
+  } else if (t < 0.75) {
+    const double u = (t - 0.5) * 4.0;
+    rgb[0] = 0.12 + (0.98 - 0.12) * u; rgb[1] = 0.82 + (0.62 - 0.82) * u; rgb[2] = 0.38 + (0.08 - 0.38) * u;
+  } else {
+    const double u = (t - 0.75) * 4.0;
+    rgb[0] = 0.98 + (0.94 - 0.98) * u; rgb[1] = 0.62 + (0.16 - 0.62) * u; rgb[2] = 0.08 + (0.18 - 0.08) * u;
+  }
+}
+
+// axis 0 = x, 1 = y, 2 = z; mode 0 = velocity, 1 = vorticity, 2 = pressure (Cp).  rho is
+// read with the pending mean-density rescale applied, as the reference's array holds it.
+__global__ void slice_kernel(const float* __restrict__ mux, const float* __restrict__ muy,
+                             const float* __restrict__ muz, const float* __restrict__ mrho,
+                             const uint8_t* __restrict__ cls, const StepState* st, int prev_slot, const Layout L,
+                             int axis, int fixed, int mode, double uref, int width, int height,
+                             uint8_t* __restrict__ rgba) {
+  const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
+  const double corr = apply ? st->corr[prev_slot] : 1.0;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const long long P = (long long)width * height;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+    const int u = (int)(p % width), v = (int)(p / width);
+    int ix = u, iy = v, iz = fixed;
+    if (axis == 1) { ix = u; iy = fixed; iz = v; }
+    else if (axis == 0) { ix = fixed; iy = v; iz = u; }
+    const long long idx = ix + (long long)nx * (iy + (long long)ny * iz);
+    uint8_t* px = rgba + p * 4;
+    if ((cls[L.cls_at(idx)] & CLS_FLAG_MASK) == CELL_SOLID) {
+      px[0] = px[1] = px[2] = px[3] = 0;
+      continue;
+    }
+    double sn = 0.5, alpha = 215.0;
+    if (mode == 0) {
+      const double a = mux[idx], b = muy[idx], c = muz[idx];
+      const double sp = sqrt(a * a + b * b + c * c);
+      sn = js_min(1.0, js_max(0.0, sp / (uref * 1.55)));
+    } else if (mode == 1) {
+      const int ixP = ix + 1 < nx ? ix + 1 : nx - 1, ixM = ix > 0 ? ix - 1 : 0;
+      const int iyP = iy + 1 < ny ? iy + 1 : ny - 1, iyM = iy > 0 ? iy - 1 : 0;
+      const int izP = iz + 1 < nz ? iz + 1 : nz - 1, izM = iz > 0 ? iz - 1 : 0;
+      auto at = [&](int x, int y, int z) { return x + (long long)nx * (y + (long long)ny * z); };
+      const double wx = 0.5 * ((double)muz[at(ix, iyP, iz)] - (double)muz[at(ix, iyM, iz)]) -
+                        0.5 * ((double)muy[at(ix, iy, izP)] - (double)muy[at(ix, iy, izM)]);
+      const double wy = 0.5 * ((double)mux[at(ix, iy, izP)] - (double)mux[at(ix, iy, izM)]) -
+                        0.5 * ((double)muz[at(ixP, iy, iz)] - (double)muz[at(ixM, iy, iz)]);
+      const double wz = 0.5 * ((double)muy[at(ixP, iy, iz)] - (double)muy[at(ixM, iy, iz)]) -
+                        0.5 * ((double)mux[at(ix, iyP, iz)] - (double)mux[at(ix, iyM, iz)]);
+      const double vm = sqrt(wx * wx + wy * wy + wz * wz);
+      const double vn = js_min(1.0, vm / (uref * 0.42));
+      sn = 0.35 + 0.65 * vn;
+      alpha = floor(70.0 + 175.0 * vn + 0.5);
+    } else {
+      float r = mrho[idx];
+      if (apply) r = (float)((double)r * corr);
+      const double cp = (((double)r - 1.0) / 3.0) / (0.5 * uref * uref);
+      sn = js_min(1.0, js_max(0.0, (cp + 1.1) / 2.1));
+    }
+    double rgb[3];
+    cfd_colormap(sn, rgb);
+    px[0] = (uint8_t)(int)floor(rgb[0] * 255.0 + 0.5);
+    px[1] = (uint8_t)(int)floor(rgb[1] * 255.0 + 0.5);
+    px[2] = (uint8_t)(int)floor(rgb[2] * 255.0 + 0.5);
+    px[3] = (uint8_t)(int)alpha;
+  }
+}
+
 }  // namespace aerosim

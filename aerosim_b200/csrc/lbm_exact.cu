@@ -140,4 +140,14 @@ cudaError_t launch_mass_stats(const float* mux, const float* muy, const float* m
   return cudaGetLastError();
 }
 
+cudaError_t launch_slice(const float* mux, const float* muy, const float* muz, const float* mrho,
+                         const uint8_t* cls, const StepState* st, int prev_slot, const Layout& L, int axis, int fixed,
+                         int mode, double uref, int width, int height, uint8_t* rgba, cudaStream_t s) {
+  const long long P = (long long)width * height;
+  const int grid = (int)std::min<long long>((P + 255) / 256, 1184);
+  slice_kernel<<<grid, 256, 0, s>>>(mux, muy, muz, mrho, cls, st, prev_slot, L, axis, fixed, mode, uref, width,
+                                    height, rgba);
+  return cudaGetLastError();
+}
+
 }  // namespace aerosim

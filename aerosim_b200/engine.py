@@ -284,9 +284,21 @@ class LBMEngine:
         self._h.call("aerosim_last_step_timing", C.byref(ms), C.byref(n))
         return ms.value, n.value
 
-    def step_and_extract_slice(self, substeps: int = 4, read_macro_field: bool = False):
-        """stepAndExtractSlice (lbmEngine.ts:404-675) without the slice image: runs
-        `substeps` steps, integrates the forces on the device and feeds the tracker."""
+    def extract_slice_rgba(self, axis: str = "z", fraction: float = 0.5, mode: str = "velocity") -> dict:
+        """extractSliceRGBA (lbmCpuReference.ts:499-596) of the last step's macro fields:
+        {'width', 'height', 'rgba'} with rgba uint8 [height * width * 4]."""
+        a = {"x": 0, "y": 1, "z": 2}[axis]
+        m = {"velocity": 0, "vorticity": 1, "pressure": 2}[mode]
+        w, h = C.c_int32(), C.c_int32()
+        self._h.call("aerosim_extract_slice", a, float(fraction), m, None, C.byref(w), C.byref(h))
+        rgba = np.empty(w.value * h.value * 4, np.uint8)
+        self._h.call("aerosim_extract_slice", a, float(fraction), m, N.ptr(rgba, C.c_uint8), C.byref(w), C.byref(h))
+        return {"width": w.value, "height": h.value, "rgba": rgba}
+
+    def step_and_extract_slice(self, substeps: int = 4, read_macro_field: bool = False, slice: dict | None = None):
+        """stepAndExtractSlice (lbmEngine.ts:404-675): runs `substeps` steps, integrates
+        the forces on the device and feeds the tracker; with `slice` ({'axis',
+        'fraction', 'mode'}) also the slice image (width, height, rgba)."""
         if not self._has_grid:
             return None
         self.step(substeps)
@@ -295,6 +307,9 @@ class LBMEngine:
         readout = self.force_tracker.push_sample(f.step, f.cd, f.cl, f.cm, f.xcp, c["windSpeedMps"],
                                                  c["fluid"], c["frontalAreaM2"])
         out = {"stepCount": int(f.step), "forceReadout": readout, "forces": f}
+        if slice is not None:
+            out.update(self.extract_slice_rgba(slice.get("axis", "z"), slice.get("fraction", 0.5),
+                                               slice.get("mode", "velocity")))
         if read_macro_field:
             out["macroField"] = self.read_macro()
         return out

@@ -183,19 +183,22 @@ def run_ours(args) -> dict:
     # ---- e2e: frames of 4 substeps + force readout to the host through the C-ABI ----
     frames = max(4, args.steps // 4) if not args.no_e2e else 0
     if frames:
+        sl = {"axis": "z", "fraction": 0.5, "mode": "velocity"}
         for _ in range(2):
-            eng.step_and_extract_slice(4)
+            eng.step_and_extract_slice(4, slice=sl)
         barrier_sync()
         t0 = time.perf_counter()
         for _ in range(frames):
-            eng.step_and_extract_slice(4)
+            fr = eng.step_and_extract_slice(4, slice=sl)
         dt = time.perf_counter() - t0
         barrier_sync()
         dt = max_over_ranks(dt)
         import ctypes
+        frame_d2h = ctypes.sizeof(N.Forces) + 4 + fr["rgba"].nbytes
         out["e2e"] = {"value": round(ws * cells * 4 * frames / dt / 1e6, 1), "unit": "MLUPS",
-                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": ctypes.sizeof(N.Forces) + 4,
-                      "frame": "aerosim_step(4 substeps) + aerosim_read_forces (FP64 sums, host copy)",
+                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": frame_d2h // 4,
+                      "frame": "stepAndExtractSlice: aerosim_step(4 substeps) + aerosim_read_forces (FP64 sums) "
+                               "+ aerosim_extract_slice (z = nz/2 velocity RGBA), results copied to the host",
                       "frames": frames}
     eng.close()
 

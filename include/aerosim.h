@@ -163,6 +163,13 @@ int aerosim_read_populations(aerosim_engine* h, void* f, int32_t dtype);
 int aerosim_write_populations(aerosim_engine* h, const void* f, int32_t dtype);
 /* computeFluidMassStats, lbmCpuReference.ts:461-495. */
 int aerosim_mass_stats(aerosim_engine* h, aerosim_mass* out);
+/* extractSliceRGBA(axis, sliceFraction, fieldMode) of the macro fields of the last step
+ * (src/solver/lbmCpuReference.ts:499-596, the image stepAndExtractSlice returns,
+ * src/solver/lbmEngine.ts:548-553): axis 0 = x (width nz, height ny), 1 = y (nx, nz),
+ * 2 = z (nx, ny); mode 0 = velocity, 1 = vorticity, 2 = pressure coefficient.  rgba:
+ * width * height * 4 bytes, row v at v * width * 4; NULL only reports the size. */
+int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fraction, int32_t mode, uint8_t* rgba,
+                          int32_t* width, int32_t* height);
 
 /* ---- timing support -------------------------------------------------------- */
 

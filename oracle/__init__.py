@@ -233,6 +233,25 @@ class Solver:
         return {"totalMass": o[0], "meanRho": o[1], "maxSpeed": o[2], "hasNaN": bool(o[3])}
 
 
+def colormap(t: float) -> tuple[float, float, float]:
+    """sampleCFDColormap (lbmCpuReference.ts:23-46)."""
+    o = np.empty(3)
+    lib().orc_colormap(C.c_double(t), _p(o, C.c_double))
+    return float(o[0]), float(o[1]), float(o[2])
+
+
+def extract_slice(solver: "Solver", axis: str, fraction: float, mode: str) -> np.ndarray:
+    """extractSliceRGBA (lbmCpuReference.ts:499-596): uint8 [height][width][4]."""
+    a = {"x": 0, "y": 1, "z": 2}[axis]
+    m = {"velocity": 0, "vorticity": 1, "pressure": 2}[mode]
+    w, h = C.c_int(), C.c_int()
+    lib().orc_extract_slice(solver.h, a, C.c_double(fraction), m, None, C.byref(w), C.byref(h))
+    out = np.zeros((h.value, w.value, 4), np.uint8)
+    lib().orc_extract_slice(solver.h, a, C.c_double(fraction), m, out.ctypes.data_as(C.POINTER(C.c_uint8)),
+                            C.byref(w), C.byref(h))
+    return out
+
+
 def momentum_exchange(vox: Voxel, f: np.ndarray) -> dict:
     """integrateLatticeMomentumExchange raw sums (forceIntegrator.ts:159-216)."""
     o = np.empty(7)

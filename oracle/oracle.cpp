@@ -1055,4 +1055,82 @@ int orc_max_threads() {
 #endif
 }
 
+// ---- slice image: sampleCFDColormap + extractSliceRGBA, lbmCpuReference.ts:23-46, 499-596
+static void cfd_colormap(double tv, double rgb[3]) {
+  const double t = js_max(0.0, js_min(1.0, tv));
+  if (t < 0.25) {
+    const double u = t * 4.0;
+    rgb[0] = 0.08 + (0.06 - 0.08) * u; rgb[1] = 0.22 + (0.72 - 0.22) * u; rgb[2] = 0.75 + (0.88 - 0.75) * u;
+  } else if (t < 0.5) {
+    const double u = (t - 0.25) * 4.0;
+    rgb[0] = 0.06 + (0.12 - 0.06) * u; rgb[1] = 0.72 + (0.82 - 0.72) * u; rgb[2] = 0.88 + (0.38 - 0.88) * u;
+  } else if (t < 0.75) {
+    const double u = (t - 0.5) * 4.0;
+    rgb[0] = 0.12 + (0.98 - 0.12) * u; rgb[1] = 0.82 + (0.62 - 0.82) * u; rgb[2] = 0.38 + (0.08 - 0.38) * u;
+  } else {
+    const double u = (t - 0.75) * 4.0;
+    rgb[0] = 0.98 + (0.94 - 0.98) * u; rgb[1] = 0.62 + (0.16 - 0.62) * u; rgb[2] = 0.08 + (0.18 - 0.08) * u;
+  }
+}
+// Math.round: the nearest integer, halves toward +infinity
+static double js_round(double x) { return std::floor(x + 0.5); }
+
+void orc_colormap(double t, double* rgb) { cfd_colormap(t, rgb); }
+
+// axis 0 = x, 1 = y, 2 = z; mode 0 = velocity, 1 = vorticity, 2 = pressure.
+// rgba: width * height * 4 bytes (width, height as the reference forms them).
+void orc_extract_slice(void* s, int axis, double frac, int mode, uint8_t* rgba, int* w_out, int* h_out) {
+  const Solver* S = (const Solver*)s;
+  const int nx = S->nx, ny = S->ny, nz = S->nz;
+  int width = nx, height = ny;
+  if (axis == 1) { width = nx; height = nz; }
+  else if (axis == 0) { width = nz; height = ny; }
+  *w_out = width;
+  *h_out = height;
+  if (!rgba) return;
+  const double uref = js_max(1e-4, S->u_inlet);
+  const int fz = (int)js_min(nz - 1, js_max(0, std::floor(frac * nz)));
+  const int fy = (int)js_min(ny - 1, js_max(0, std::floor(frac * ny)));
+  const int fx = (int)js_min(nx - 1, js_max(0, std::floor(frac * nx)));
+  const float *ux = S->ux.data(), *uy = S->uy.data(), *uz = S->uz.data(), *rho = S->rho.data();
+  for (int v = 0; v < height; ++v)
+    for (int u = 0; u < width; ++u) {
+      int ix = u, iy = v, iz = fz;
+      if (axis == 1) { ix = u; iy = fy; iz = v; }
+      else if (axis == 0) { ix = fx; iy = v; iz = u; }
+      const int64_t idx = ix + (int64_t)nx * (iy + (int64_t)ny * iz);
+      uint8_t* px = rgba + ((int64_t)v * width + u) * 4;
+      if (S->flags[idx] == CELL_SOLID) { px[0] = px[1] = px[2] = px[3] = 0; continue; }
+      double sn = 0.5, alpha = 215;
+      if (mode == 0) {
+        const double sp = std::sqrt((double)ux[idx] * ux[idx] + (double)uy[idx] * uy[idx] + (double)uz[idx] * uz[idx]);
+        sn = js_min(1.0, js_max(0.0, sp / (uref * 1.55)));
+      } else if (mode == 1) {
+        const int ixP = (int)js_min(nx - 1, ix + 1), ixM = (int)js_max(0, ix - 1);
+        const int iyP = (int)js_min(ny - 1, iy + 1), iyM = (int)js_max(0, iy - 1);
+        const int izP = (int)js_min(nz - 1, iz + 1), izM = (int)js_max(0, iz - 1);
+        auto at = [&](int x, int y, int z) { return x + (int64_t)nx * (y + (int64_t)ny * z); };
+        const double wx = 0.5 * ((double)uz[at(ix, iyP, iz)] - uz[at(ix, iyM, iz)]) -
+                          0.5 * ((double)uy[at(ix, iy, izP)] - uy[at(ix, iy, izM)]);
+        const double wy = 0.5 * ((double)ux[at(ix, iy, izP)] - ux[at(ix, iy, izM)]) -
+                          0.5 * ((double)uz[at(ixP, iy, iz)] - uz[at(ixM, iy, iz)]);
+        const double wz = 0.5 * ((double)uy[at(ixP, iy, iz)] - uy[at(ixM, iy, iz)]) -
+                          0.5 * ((double)ux[at(ix, iyP, iz)] - ux[at(ix, iyM, iz)]);
+        const double vm = std::sqrt(wx * wx + wy * wy + wz * wz);
+        const double vn = js_min(1.0, vm / (uref * 0.42));
+        sn = 0.35 + 0.65 * vn;
+        alpha = js_round(70 + 175 * vn);
+      } else {
+        const double cp = (((double)rho[idx] - 1.0) / 3.0) / (0.5 * uref * uref);
+        sn = js_min(1.0, js_max(0.0, (cp + 1.1) / 2.1));
+      }
+      double rgb[3];
+      cfd_colormap(sn, rgb);
+      px[0] = (uint8_t)(int)js_round(rgb[0] * 255);
+      px[1] = (uint8_t)(int)js_round(rgb[1] * 255);
+      px[2] = (uint8_t)(int)js_round(rgb[2] * 255);
+      px[3] = (uint8_t)(int)alpha;
+    }
+}
+
 }  // extern "C"

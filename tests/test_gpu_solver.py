@@ -276,3 +276,25 @@ def test_engines_sharing_a_kernel_with_different_rings(gpu_engine_cls, oracle_mo
         for eng in engines:
             eng.step(3)
     assert [e.get_step_count() for e in engines] == [6, 6]
+
+
+@pytest.mark.parametrize("precision", ["f32_mirror", "f32"])
+def test_slice_images_match_the_oracle(gpu_engine_cls, oracle_mod, precision):
+    """extractSliceRGBA on the three axes and the three field modes after 150 steps:
+    byte-identical to the oracle in the bit-parity mode; in FP32 at most a few pixels
+    one colour level apart."""
+    case = cases.sphere_64x32x32()
+    vox, orc, eng = _pair(gpu_engine_cls, oracle_mod, case, precision)
+    orc.step(150, threads=_threads(oracle_mod))
+    eng.step(150)
+    for axis in ("x", "y", "z"):
+        for mode in ("velocity", "vorticity", "pressure"):
+            ref = oracle_mod.extract_slice(orc, axis, 0.45, mode)
+            got = eng.extract_slice_rgba(axis, 0.45, mode)
+            img = got["rgba"].reshape(got["height"], got["width"], 4)
+            assert img.shape == ref.shape
+            diff = np.abs(img.astype(int) - ref.astype(int))
+            if precision == "f32_mirror":
+                assert diff.max() == 0, (axis, mode)
+            else:
+                assert diff.max() <= 2 and np.mean(diff > 0) < 0.01, (axis, mode, diff.max())

@@ -215,3 +215,14 @@ def test_cd_band(oracle_mod, name):
     assert lo <= cd <= hi, (name, cd, lo, hi, re)
     if name in ("cube", "sphere"):
         assert abs(round(out["meanCl"], 3)) <= 0.02
+
+
+def test_colormap_knots():
+    """sampleCFDColormap (lbmCpuReference.ts:23-46): the four segment ends, clamping."""
+    import oracle
+    assert oracle.colormap(0.0) == (0.08, 0.22, 0.75)
+    assert oracle.colormap(-1.0) == (0.08, 0.22, 0.75)
+    r, g, b = oracle.colormap(0.5)
+    assert abs(r - 0.12) < 1e-15 and abs(g - 0.82) < 1e-15 and abs(b - 0.38) < 1e-15
+    r, g, b = oracle.colormap(2.0)
+    assert abs(r - 0.94) < 1e-15 and abs(g - 0.16) < 1e-15 and abs(b - 0.18) < 1e-15
