@@ -218,6 +218,32 @@ def run_ours(args) -> dict:
                                   "frac": round(ach2 / hbm, 4), "traffic": _profile_traffic(prec)}}
         e2.close()
 
+    # ---- learned SGS closure (trained weights shipped with the package) ----
+    wpath = os.path.join(ROOT, "aerosim_b200", "data", "sgs_mlp_ellipsoid.npz")
+    if args.sgs_steps > 0 and os.path.exists(wpath):
+        w = np.load(wpath)
+        e4, _ = _make_engine(case, "f32", dev)
+        e4.set_sgs_mlp(w["params"])
+        e4.step(args.warmup)
+        barrier_sync()
+        ms4, l4 = _timed_steps(e4, args.sgs_steps)
+        barrier_sync()
+        ms4 = max_over_ranks(ms4)
+        nan = e4.mass_stats()["hasNaN"]
+        e4.close()
+        meta = {}
+        mpath = wpath.replace(".npz", ".json")
+        if os.path.exists(mpath):
+            with open(mpath) as f:
+                meta = json.load(f)
+        out["sgs_closure"] = {
+            "mlups": round(ws * cells * args.sgs_steps / (ms4 * 1e-3) / 1e6, 1), "ms_per_step": ms4 / args.sgs_steps,
+            "vs_smagorinsky_time": round((ms4 / args.sgs_steps) / (ms / args.steps), 3), "gpu_launches": int(l4),
+            "nan": nan, "inference": "BF16 mma.sync m16n8k16 tiles, FP32 accumulation, inside the step kernel",
+            "training": {k: meta[k] for k in ("fine", "coarse", "fine_cd_mean", "heldout_mse_mlp",
+                                               "heldout_mse_smagorinsky", "coarse_smagorinsky", "coarse_mlp")
+                         if k in meta}}
+
     # ---- batched sweep: 32 wings of uneven lattice sizes, one launch per step ----
     if args.batch_steps > 0:
         out["batch"] = run_batch(args, dev, ws, barrier_sync, max_over_ranks)
@@ -391,6 +417,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cd-steps", type=int, default=20000, help="steps of the FP64-oracle Cd comparison (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--sgs-steps", type=int, default=2000,
+                    help="steps of the 256x128x128 case with the learned closure (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=10000,
                     help="steps of the batched 32-wing sweep (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
