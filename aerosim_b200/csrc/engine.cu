@@ -974,6 +974,7 @@ struct aerosim_batch {
   void** d_bufs = nullptr;
   long long* d_item_begin = nullptr;
   long long* d_near_begin = nullptr;
+  int4* d_geo = nullptr;
   unsigned long long* d_partials = nullptr;
   unsigned int* d_ticket = nullptr;  // [2]
   int* d_step = nullptr;
@@ -1007,6 +1008,7 @@ void batch_free(aerosim_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   cudaFree(b->d_inst); cudaFree(b->d_bufs); cudaFree(b->d_item_begin); cudaFree(b->d_near_begin);
+  cudaFree(b->d_geo);
   cudaFree(b->d_partials); cudaFree(b->d_ticket); cudaFree(b->d_step); cudaFree(b->d_error);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -1038,6 +1040,7 @@ BatchArgs batch_args(const aerosim_batch* b, int write_macro) {
   BatchArgs a{};
   a.inst = b->d_inst; a.bufs = b->d_bufs; a.item_begin = b->d_item_begin; a.near_begin = b->d_near_begin;
   a.partials = b->d_partials; a.ticket = b->d_ticket; a.step = b->d_step; a.error = b->d_error;
+  a.geo = b->d_geo;
   a.n_items = b->n_items; a.n_near = b->n_near; a.slot_elems = b->slot_elems; a.slot_cls = b->slot_cls;
   a.n_inst = (int)b->eng.size(); a.stages = b->tune.stages; a.write_macro = write_macro;
   return a;
@@ -1170,6 +1173,7 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
   cudaError_t e = cudaSetDevice(b->device);
   std::vector<long long> item_begin(n + 1, 0), near_begin(n + 1, 0);
   std::vector<void*> bufs(2 * (size_t)n);
+  std::vector<int4> geo(n);
   int pitch = engines[0]->L.pitch;
   for (int k = 0; k < n; ++k) {
     const aerosim_engine* en = engines[k];
@@ -1178,6 +1182,7 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
     const long long rows = (long long)L.ny * L.nz;
     item_begin[k + 1] = item_begin[k] + (rows + RY - 1) / RY;
     near_begin[k + 1] = near_begin[k] + en->n_near;
+    geo[k] = make_int4(RY, (L.nx + row_shift(L.nx) + 31) / 32, row_shift(L.nx), 0);
     bufs[2 * k] = en->f[0];
     bufs[2 * k + 1] = en->f[1];
     b->slot_elems = std::max<long long>(b->slot_elems, (long long)RY * 19 * L.pitch);
@@ -1196,6 +1201,7 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
   if (e == cudaSuccess) e = cudaMalloc(&b->d_bufs, 2 * n * sizeof(void*));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_item_begin, (n + 1) * sizeof(long long));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_near_begin, (n + 1) * sizeof(long long));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_geo, n * sizeof(int4));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_partials, part * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_ticket, 2 * sizeof(unsigned int));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_step, sizeof(int));
@@ -1206,6 +1212,7 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
     e = cudaMemcpy(b->d_item_begin, item_begin.data(), item_begin.size() * sizeof(long long), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_near_begin, near_begin.data(), near_begin.size() * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_geo, geo.data(), geo.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     bfail(AEROSIM_ERR_CUDA, std::string("batch_create: ") + cudaGetErrorString(e));
     return bail(AEROSIM_ERR_CUDA);

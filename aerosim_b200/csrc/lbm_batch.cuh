@@ -23,6 +23,7 @@ struct BatchArgs {
   const long long* near_begin;   // [n_inst + 1] first near-wall cell of each instance
   unsigned long long* partials;  // [gridDim.x * n_inst] per-CTA fixed-point density sums
   unsigned int* ticket;          // [2] CTAs done, per step parity
+  const int4* geo;               // [n_inst] rows per item, 32-cell segments per row, row shift
   int* step;                     // step counter shared by all instances
   int* error;                    // pipeline timeout flag of the batch
   long long n_items, n_near;
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
       const StepArgs& ia = b.inst[k];
       const int nx = ia.L.nx, ny = ia.L.ny, nz = ia.L.nz;
       const int pitch = P ? P : ia.L.pitch;
-      const int RY = rows_per_item(nx);
+      const int RY = b.geo[k].x;
       const long long rows = (long long)ny * nz;
       const long long r0 = (gi - b.item_begin[k]) * RY;
       const int nr = (int)(rows - r0 < RY ? rows - r0 : RY);
@@ -211,8 +212,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
       const StepArgs& ia = b.inst[k];
       const int nx = ia.L.nx, ny = ia.L.ny, nz = ia.L.nz;
       const int pitch = P ? P : ia.L.pitch;
-      const int shift = row_shift(nx), RY = rows_per_item(nx);
-      const int segs = (nx + shift + 31) / 32;  // segments per row
+      const int4 geo = b.geo[k];
+      const int RY = geo.x, segs = geo.y, shift = geo.z;  // rows per item, segments per row, shift
       const long long rows = (long long)ny * nz;
       const long long row0 = (gi - b.item_begin[k]) * RY;
       const int nr = (int)(rows - row0 < RY ? rows - row0 : RY);
@@ -232,9 +233,9 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
       T* fd = static_cast<T*>(b.bufs[2 * k + (cur ^ 1)]);
       long long item_sum = 0;
       int my_nan = 0;
+      int ry = first / segs, sr = first - ry * segs;  // row and segment of segment `sg`
       for (int sg = first; sg < total; sg += kConsumerWarps) {
-        const int ry = sg / segs;
-        const int cell_lo = (sg - ry * segs) * 32 - shift;
+        const int cell_lo = sr * 32 - shift;
         const int2 yz = s_row[s * kMaxRowsPerItem + ry];
         const int iy = yz.x, iz = yz.y;
         const T* sp = spop + (size_t)s * b.slot_elems + (size_t)ry * 19 * pitch;
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
                           return make_float2((float)u.x, (float)u.y);
                         },
                         ia, s_xo + warp * 20, s_dcw, s_dslot, lane, item_sum, my_nan);
+        for (sr += kConsumerWarps; sr >= segs; sr -= segs) ++ry;
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) item_sum += __shfl_down_sync(0xffffffffu, item_sum, o);
