@@ -325,8 +325,8 @@ int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[
   h->dx = dx;
   h->origin[0] = origin[0]; h->origin[1] = origin[1]; h->origin[2] = origin[2];
   h->fluid_count = h->g.N - h->g.solid;
-  // force reduction: 8 boundary cells per CTA and round, at most 8 CTAs per SM
-  const long long blocks = std::max<long long>(1, std::min<long long>((h->g.B + 7) / 8, 8LL * h->num_sms));
+  // force reduction: 8 boundary cells per CTA and round, at most 2 CTAs per SM
+  const long long blocks = std::max<long long>(1, std::min<long long>((h->g.B + 7) / 8, 2LL * h->num_sms));
   if (blocks > h->force_blocks_cap) {
     cudaFree(h->force_partials);
     h->force_partials = nullptr;

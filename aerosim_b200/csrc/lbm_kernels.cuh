@@ -1247,13 +1247,16 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
   }
   __syncthreads();
   if (is_last) {
+    // component k by warp k: lanes stride over the CTAs' partials, then a shuffle tree
+    // (a fixed order, so the total does not depend on which CTA finished last)
     __threadfence();
-    if (threadIdx.x < 7) {
+    if (warp < 7) {
       double s = 0.0;
-      for (unsigned int blk = 0; blk < gridDim.x; ++blk) {
-        s += *(volatile double*)&a.partials[(long long)blk * 8 + threadIdx.x];
-      }
-      a.out[threadIdx.x] = s;
+      for (unsigned int blk = lane; blk < gridDim.x; blk += 32)
+        s += __ldcg(&a.partials[(long long)blk * 8 + warp]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) a.out[warp] = s;
     }
     if (threadIdx.x == 0) {
       a.out[7] = (double)gridDim.x;
