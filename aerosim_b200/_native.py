@@ -101,6 +101,9 @@ SIGNATURES = {
     "aerosim_write_populations": ([_P, _P, C.c_int32], C.c_int),
     "aerosim_extract_slice": ([_P, C.c_int32, C.c_double, C.c_int32, _U8P, C.POINTER(C.c_int32),
                                C.POINTER(C.c_int32)], C.c_int),
+    "aerosim_q_criterion": ([_P, _F32P, _F32P, _F32P, _F64P, _F64P], C.c_int),
+    "aerosim_q_criterion_fields": ([_P, C.c_int32, C.c_int32, C.c_int32, C.c_double, _F32P, _F32P, _F32P, _U8P,
+                                    _F32P, _F32P, _F32P, _F64P, _F64P], C.c_int),
     "aerosim_mass_stats": ([_P, C.POINTER(Mass)], C.c_int),
     "aerosim_last_step_timing": ([_P, _F64P, C.POINTER(C.c_int64)], C.c_int),
     "aerosim_batch_create": ([C.POINTER(_P), C.c_int32, C.POINTER(_P)], C.c_int),

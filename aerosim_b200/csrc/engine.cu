@@ -861,6 +861,69 @@ extern "C" int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fra
   return AEROSIM_OK;
 }
 
+namespace {
+
+// Q-criterion of device velocity fields into host outputs (staging: 5 floats per cell).
+int q_criterion_to_host(aerosim_engine* h, int nx, int ny, int nz, double dx, const float* ux, const float* uy,
+                        const float* uz, const uint8_t* flags, float* q, float* om, float* omv, double* max_q,
+                        double* max_om) {
+  const long long N = (long long)nx * ny * nz;
+  int rc = ensure_staging(h, N * 5 * sizeof(float) + 16);
+  if (rc) return rc;
+  float* dq = static_cast<float*>(h->staging);
+  float* dom = dq + N;
+  float* domv = dom + N;
+  unsigned long long* dmax = h->stats_buf;
+  CU(h, launch_q_criterion(nx, ny, nz, dx, ux, uy, uz, flags, dq, dom, domv, dmax, h->stream));
+  unsigned long long mx[2] = {0, 0};
+  if (q) CU(h, cudaMemcpyAsync(q, dq, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  if (om) CU(h, cudaMemcpyAsync(om, dom, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  if (omv) CU(h, cudaMemcpyAsync(omv, domv, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaMemcpyAsync(mx, dmax, sizeof(mx), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  double a, b;
+  std::memcpy(&a, &mx[0], 8);
+  std::memcpy(&b, &mx[1], 8);
+  if (max_q) *max_q = std::max(1e-6, a);
+  if (max_om) *max_om = std::max(1e-6, b);
+  return AEROSIM_OK;
+}
+
+}  // namespace
+
+extern "C" int aerosim_q_criterion(aerosim_engine* h, float* q, float* omega_mag, float* omega_vec, double* max_q,
+                                   double* max_omega) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "q_criterion: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  return q_criterion_to_host(h, h->g.nx, h->g.ny, h->g.nz, h->dx, h->mux, h->muy, h->muz, h->g.flags, q, omega_mag,
+                             omega_vec, max_q, max_omega);
+}
+
+extern "C" int aerosim_q_criterion_fields(aerosim_engine* h, int32_t nx, int32_t ny, int32_t nz, double dx,
+                                          const float* ux, const float* uy, const float* uz, const uint8_t* flags,
+                                          float* q, float* omega_mag, float* omega_vec, double* max_q,
+                                          double* max_omega) {
+  if (!h || !ux || !uy || !uz || nx < 1 || ny < 1 || nz < 1 || !(dx > 0.0))
+    return fail(h, AEROSIM_ERR_ARG, "q_criterion_fields: bad argument");
+  CU(h, cudaSetDevice(h->device));
+  const long long N = (long long)nx * ny * nz;
+  void* buf = nullptr;
+  CU(h, cudaMalloc(&buf, N * (3 * sizeof(float) + 1)));
+  float* d = static_cast<float*>(buf);
+  uint8_t* df = reinterpret_cast<uint8_t*>(d + 3 * N);
+  cudaError_t e = cudaMemcpyAsync(d, ux, N * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d + N, uy, N * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d + 2 * N, uz, N * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && flags) e = cudaMemcpyAsync(df, flags, N, cudaMemcpyHostToDevice, h->stream);
+  int rc = e == cudaSuccess ? q_criterion_to_host(h, nx, ny, nz, dx, d, d + N, d + 2 * N, flags ? df : nullptr, q,
+                                                  omega_mag, omega_vec, max_q, max_omega)
+                            : fail(h, AEROSIM_ERR_CUDA, std::string("q_criterion_fields: ") + cudaGetErrorString(e));
+  cudaStreamSynchronize(h->stream);
+  cudaFree(buf);
+  return rc;
+}
+
 // ---------------------------------------------------------------------------
 // Learned SGS closure of an engine.
 // ---------------------------------------------------------------------------

@@ -70,6 +70,12 @@ cudaError_t launch_slice(const float* mux, const float* muy, const float* muz, c
                          const uint8_t* cls, const StepState* st, int prev_slot, const Layout& L, int axis, int fixed,
                          int mode, double uref, int width, int height, uint8_t* rgba, cudaStream_t s);
 
+// computeQCriterion over dense float velocity fields (flags may be null); maxima[2]
+// receive the bit patterns of max Q and max |omega| before the reference's 1e-6 floor.
+cudaError_t launch_q_criterion(int nx, int ny, int nz, double dx, const float* ux, const float* uy, const float* uz,
+                               const uint8_t* flags, float* q, float* om, float* omv, unsigned long long* maxima,
+                               cudaStream_t s);
+
 // sgs.cu: jump-flood wall distance of a dense flag array into float distances (dist,
 // may be null) and bits 3..7 of the pitched class bytes (cls, may be null); training
 // samples of the learned closure from a fine flow's macro fields and a 2x coarser grid.

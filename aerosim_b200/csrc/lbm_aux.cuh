@@ -254,4 +254,57 @@ __global__ void slice_kernel(const float* __restrict__ mux, const float* __restr
   }
 }
 
+// ---- Q-criterion and vorticity, src/render/vortexIso.ts:22-122: FP64 per cell in the
+// reference's operation order (-fmad=false), float outputs, 0 at solid cells (flags may be
+// null); the maxima (starting at 1e-6) as the bit patterns of non-negative doubles, so an
+// unsigned max is exact and order-free.
+__global__ void q_criterion_kernel(int nx, int ny, int nz, double dx, const float* __restrict__ ux,
+                                   const float* __restrict__ uy, const float* __restrict__ uz,
+                                   const uint8_t* __restrict__ flags, float* __restrict__ q,
+                                   float* __restrict__ om, float* __restrict__ omv,
+                                   unsigned long long* __restrict__ maxima) {
+  const long long N = (long long)nx * ny * nz;
+  const double inv2dx = 1.0 / (2.0 * dx);
+  double mq = 0.0, mo = 0.0;
+  auto at = [&](int x, int y, int z) { return x + (long long)nx * (y + (long long)ny * z); };
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % nx);
+    const long long r = i / nx;
+    const int iy = (int)(r % ny), iz = (int)(r / ny);
+    if (flags && flags[i] == CELL_SOLID) {
+      q[i] = 0.0f; om[i] = 0.0f; omv[3 * i] = 0.0f; omv[3 * i + 1] = 0.0f; omv[3 * i + 2] = 0.0f;
+      continue;
+    }
+    const int xp = ix > 0 ? ix - 1 : 0, xn = ix + 1 < nx ? ix + 1 : nx - 1;
+    const int yp = iy > 0 ? iy - 1 : 0, yn = iy + 1 < ny ? iy + 1 : ny - 1;
+    const int zp = iz > 0 ? iz - 1 : 0, zn = iz + 1 < nz ? iz + 1 : nz - 1;
+    const double sx = xn > xp ? 1.0 / ((xn - xp) * dx) : inv2dx;
+    const double sy = yn > yp ? 1.0 / ((yn - yp) * dx) : inv2dx;
+    const double sz = zn > zp ? 1.0 / ((zn - zp) * dx) : inv2dx;
+    const double a = ((double)ux[at(xn, iy, iz)] - (double)ux[at(xp, iy, iz)]) * sx;
+    const double b = ((double)ux[at(ix, yn, iz)] - (double)ux[at(ix, yp, iz)]) * sy;
+    const double c = ((double)ux[at(ix, iy, zn)] - (double)ux[at(ix, iy, zp)]) * sz;
+    const double d = ((double)uy[at(xn, iy, iz)] - (double)uy[at(xp, iy, iz)]) * sx;
+    const double e = ((double)uy[at(ix, yn, iz)] - (double)uy[at(ix, yp, iz)]) * sy;
+    const double f = ((double)uy[at(ix, iy, zn)] - (double)uy[at(ix, iy, zp)]) * sz;
+    const double g = ((double)uz[at(xn, iy, iz)] - (double)uz[at(xp, iy, iz)]) * sx;
+    const double h = ((double)uz[at(ix, yn, iz)] - (double)uz[at(ix, yp, iz)]) * sy;
+    const double k = ((double)uz[at(ix, iy, zn)] - (double)uz[at(ix, iy, zp)]) * sz;
+    const double S12 = 0.5 * (b + d), S13 = 0.5 * (c + g), S23 = 0.5 * (f + h);
+    const double nS = a * a + e * e + k * k + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23);
+    const double O12 = 0.5 * (b - d), O13 = 0.5 * (c - g), O23 = 0.5 * (f - h);
+    const double nO = 2.0 * (O12 * O12 + O13 * O13 + O23 * O23);
+    const double qv = 0.5 * (nO - nS);
+    q[i] = (float)qv;
+    if (qv > mq) mq = qv;
+    const double ox = h - f, oy = c - g, oz = d - b;
+    const double m = sqrt(ox * ox + oy * oy + oz * oz);
+    omv[3 * i] = (float)ox; omv[3 * i + 1] = (float)oy; omv[3 * i + 2] = (float)oz;
+    om[i] = (float)m;
+    if (m > mo) mo = m;
+  }
+  atomicMax(&maxima[0], (unsigned long long)__double_as_longlong(mq));
+  atomicMax(&maxima[1], (unsigned long long)__double_as_longlong(mo));
+}
+
 }  // namespace aerosim

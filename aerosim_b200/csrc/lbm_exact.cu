@@ -150,4 +150,15 @@ cudaError_t launch_slice(const float* mux, const float* muy, const float* muz, c
   return cudaGetLastError();
 }
 
+cudaError_t launch_q_criterion(int nx, int ny, int nz, double dx, const float* ux, const float* uy, const float* uz,
+                               const uint8_t* flags, float* q, float* om, float* omv, unsigned long long* maxima,
+                               cudaStream_t s) {
+  const long long N = (long long)nx * ny * nz;
+  cudaError_t e = cudaMemsetAsync(maxima, 0, 2 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  const int grid = (int)std::min<long long>((N + 255) / 256, 148 * 8);
+  q_criterion_kernel<<<grid, 256, 0, s>>>(nx, ny, nz, dx, ux, uy, uz, flags, q, om, omv, maxima);
+  return cudaGetLastError();
+}
+
 }  // namespace aerosim

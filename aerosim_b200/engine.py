@@ -314,6 +314,29 @@ class LBMEngine:
             out["macroField"] = self.read_macro()
         return out
 
+    def q_criterion(self, fields: dict | None = None, dx: float | None = None) -> dict:
+        """computeQCriterion (vortexIso.ts:22-122) on the GPU: of the last step's macro
+        velocity, or of caller fields {'nx','ny','nz','ux','uy','uz'[, 'flags']} with
+        spacing dx.  Returns qValues, omegaMag, omegaVec, maxQ, maxOmega."""
+        mq, mo = C.c_double(), C.c_double()
+        if fields is None:
+            info = self.voxel_info()
+            n = info.nx * info.ny * info.nz
+            q, om, omv = np.empty(n, np.float32), np.empty(n, np.float32), np.empty(3 * n, np.float32)
+            self._h.call("aerosim_q_criterion", N.ptr(q, C.c_float), N.ptr(om, C.c_float), N.ptr(omv, C.c_float),
+                         C.byref(mq), C.byref(mo))
+        else:
+            nx, ny, nz = int(fields["nx"]), int(fields["ny"]), int(fields["nz"])
+            n = nx * ny * nz
+            u = [np.ascontiguousarray(fields[k], np.float32) for k in ("ux", "uy", "uz")]
+            fl = fields.get("flags")
+            fl = None if fl is None else np.ascontiguousarray(fl, np.uint8)
+            q, om, omv = np.empty(n, np.float32), np.empty(n, np.float32), np.empty(3 * n, np.float32)
+            self._h.call("aerosim_q_criterion_fields", nx, ny, nz, float(dx), *[N.ptr(a, C.c_float) for a in u],
+                         N.ptr(fl, C.c_uint8), N.ptr(q, C.c_float), N.ptr(om, C.c_float), N.ptr(omv, C.c_float),
+                         C.byref(mq), C.byref(mo))
+        return {"qValues": q, "omegaMag": om, "omegaVec": omv, "maxQ": mq.value, "maxOmega": mo.value}
+
     def set_sgs_mlp(self, params) -> None:
         """Learned SGS closure (aerosim_b200.sgs parameters) for the following steps;
         None restores Smagorinsky."""

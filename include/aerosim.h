@@ -196,6 +196,20 @@ int aerosim_momentum_exchange_noalloc(const float* f, const uint8_t* flags, cons
                                       const float* q, int64_t boundary_count, int32_t nx, int32_t ny,
                                       int32_t nz, double* out, void* stream);
 
+/* ---- diagnostics of the flow field ------------------------------------------ */
+
+/* computeQCriterion (src/render/vortexIso.ts:22-122) of the macro velocity of the last
+ * step: Q = (|Omega|^2 - |S|^2) / 2 per cell, the vorticity magnitude and vector
+ * (3 floats per cell), 0 at solid cells; maxima as the reference forms them (floor 1e-6).
+ * Any output pointer may be NULL. */
+int aerosim_q_criterion(aerosim_engine* h, float* q, float* omega_mag, float* omega_vec, double* max_q,
+                        double* max_omega);
+/* The same for caller velocity fields (host arrays, dense idx = ix + nx (iy + ny iz));
+ * flags (0 fluid, 1 solid, 2 boundary) may be NULL. */
+int aerosim_q_criterion_fields(aerosim_engine* h, int32_t nx, int32_t ny, int32_t nz, double dx, const float* ux,
+                               const float* uy, const float* uz, const uint8_t* flags, float* q, float* omega_mag,
+                               float* omega_vec, double* max_q, double* max_omega);
+
 /* ---- learned subgrid-scale closure ----------------------------------------- */
 
 /* A per-cell MLP (8 inputs -> 32 -> 32 -> 1, GELU; inputs: the strain rate estimated

@@ -252,6 +252,19 @@ def extract_slice(solver: "Solver", axis: str, fraction: float, mode: str) -> np
     return out
 
 
+def q_criterion(nx, ny, nz, dx, ux, uy, uz, flags=None) -> dict:
+    """computeQCriterion (vortexIso.ts:22-122)."""
+    n = nx * ny * nz
+    ux, uy, uz = (np.ascontiguousarray(a, np.float32) for a in (ux, uy, uz))
+    fl = None if flags is None else np.ascontiguousarray(flags, np.uint8)
+    q, om, omv = np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(3 * n, np.float32)
+    mq, mo = C.c_double(), C.c_double()
+    lib().orc_q_criterion(nx, ny, nz, C.c_double(dx), _p(ux, C.c_float), _p(uy, C.c_float), _p(uz, C.c_float),
+                          None if fl is None else fl.ctypes.data_as(C.POINTER(C.c_uint8)), _p(q, C.c_float),
+                          _p(om, C.c_float), _p(omv, C.c_float), C.byref(mq), C.byref(mo))
+    return {"qValues": q, "omegaMag": om, "omegaVec": omv, "maxQ": mq.value, "maxOmega": mo.value}
+
+
 def momentum_exchange(vox: Voxel, f: np.ndarray) -> dict:
     """integrateLatticeMomentumExchange raw sums (forceIntegrator.ts:159-216)."""
     o = np.empty(7)

@@ -1133,4 +1133,48 @@ void orc_extract_slice(void* s, int axis, double frac, int mode, uint8_t* rgba, 
     }
 }
 
+// ---- Q-criterion and vorticity, src/render/vortexIso.ts:22-122 (computeQCriterion).
+// flags may be null; outputs: q[N], om[N], omv[3N] (float, 0 at solid cells), maxima.
+void orc_q_criterion(int nx, int ny, int nz, double dx, const float* ux, const float* uy, const float* uz,
+                     const uint8_t* flags, float* q, float* om, float* omv, double* max_q, double* max_om) {
+  double mq = 1e-6, mo = 1e-6;
+  const double inv2dx = 1.0 / (2.0 * dx);
+  auto at = [&](int x, int y, int z) { return x + (int64_t)nx * (y + (int64_t)ny * z); };
+  for (int iz = 0; iz < nz; ++iz)
+    for (int iy = 0; iy < ny; ++iy)
+      for (int ix = 0; ix < nx; ++ix) {
+        const int64_t i = at(ix, iy, iz);
+        if (flags && flags[i] == 1) continue;
+        const int xp = (int)js_max(0, ix - 1), xn = (int)js_min(nx - 1, ix + 1);
+        const int yp = (int)js_max(0, iy - 1), yn = (int)js_min(ny - 1, iy + 1);
+        const int zp = (int)js_max(0, iz - 1), zn = (int)js_min(nz - 1, iz + 1);
+        const double sx = xn > xp ? 1.0 / ((xn - xp) * dx) : inv2dx;
+        const double sy = yn > yp ? 1.0 / ((yn - yp) * dx) : inv2dx;
+        const double sz = zn > zp ? 1.0 / ((zn - zp) * dx) : inv2dx;
+        const double a = ((double)ux[at(xn, iy, iz)] - ux[at(xp, iy, iz)]) * sx;
+        const double b = ((double)ux[at(ix, yn, iz)] - ux[at(ix, yp, iz)]) * sy;
+        const double c = ((double)ux[at(ix, iy, zn)] - ux[at(ix, iy, zp)]) * sz;
+        const double d = ((double)uy[at(xn, iy, iz)] - uy[at(xp, iy, iz)]) * sx;
+        const double e = ((double)uy[at(ix, yn, iz)] - uy[at(ix, yp, iz)]) * sy;
+        const double f = ((double)uy[at(ix, iy, zn)] - uy[at(ix, iy, zp)]) * sz;
+        const double g = ((double)uz[at(xn, iy, iz)] - uz[at(xp, iy, iz)]) * sx;
+        const double h = ((double)uz[at(ix, yn, iz)] - uz[at(ix, yp, iz)]) * sy;
+        const double k = ((double)uz[at(ix, iy, zn)] - uz[at(ix, iy, zp)]) * sz;
+        const double S12 = 0.5 * (b + d), S13 = 0.5 * (c + g), S23 = 0.5 * (f + h);
+        const double nS = a * a + e * e + k * k + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23);
+        const double O12 = 0.5 * (b - d), O13 = 0.5 * (c - g), O23 = 0.5 * (f - h);
+        const double nO = 2.0 * (O12 * O12 + O13 * O13 + O23 * O23);
+        const double qv = 0.5 * (nO - nS);
+        q[i] = (float)qv;
+        if (qv > mq) mq = qv;
+        const double ox = h - f, oy = c - g, oz = d - b;
+        const double m = std::sqrt(ox * ox + oy * oy + oz * oz);
+        omv[3 * i] = (float)ox; omv[3 * i + 1] = (float)oy; omv[3 * i + 2] = (float)oz;
+        om[i] = (float)m;
+        if (m > mo) mo = m;
+      }
+  *max_q = mq;
+  *max_om = mo;
+}
+
 }  // extern "C"

@@ -226,3 +226,26 @@ def test_colormap_knots():
     assert abs(r - 0.12) < 1e-15 and abs(g - 0.82) < 1e-15 and abs(b - 0.38) < 1e-15
     r, g, b = oracle.colormap(2.0)
     assert abs(r - 0.94) < 1e-15 and abs(g - 0.16) < 1e-15 and abs(b - 0.18) < 1e-15
+
+
+def _rotation_and_shear():
+    nx = ny = nz = 16
+    dx = 0.1
+    iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    cx, cy = (nx - 1) / 2, (ny - 1) / 2
+    rot = (-5.0 * (iy - cy) * dx, 5.0 * (ix - cx) * dx, np.zeros_like(ix, float))
+    shear = (4.0 * (iy * dx), np.zeros_like(ix, float), np.zeros_like(ix, float))
+    return nx, ny, nz, dx, rot, shear
+
+
+def test_q_criterion_known_answers():
+    """phase5.test.ts:13-84: solid-body rotation (Q = omega0^2 = 25, |curl u| = 10 at
+    the centre) and simple shear (Q = 0)."""
+    import oracle
+    nx, ny, nz, dx, rot, shear = _rotation_and_shear()
+    mid = nx // 2 + nx * (ny // 2 + ny * (nz // 2))
+    r = oracle.q_criterion(nx, ny, nz, dx, *[a.astype(np.float32).ravel() for a in rot])
+    assert 20.0 < r["qValues"][mid] <= 25.5
+    assert abs(r["omegaMag"][mid] - 10.0) < 0.5
+    s = oracle.q_criterion(nx, ny, nz, dx, *[a.astype(np.float32).ravel() for a in shear])
+    assert abs(s["qValues"][mid]) < 1e-4
