@@ -15,7 +15,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("AEROSIM_LIB", os.path.join(_HERE, "lib", "libaerosim.so"))
 
 OK = 0
-ERR_ARG, ERR_STATE, ERR_CUDA, ERR_DEVICE, ERR_NOMEM = -1, -2, -3, -4, -5
+ERR_ARG, ERR_STATE, ERR_CUDA, ERR_DEVICE, ERR_NOMEM, ERR_FORMAT = -1, -2, -3, -4, -5, -6
+
+STL_BINARY, STL_ASCII = 0, 1
 
 CELL_FLUID, CELL_SOLID, CELL_BOUNDARY = 0, 1, 2
 
@@ -72,6 +74,16 @@ class BatchTuning(C.Structure):
                 ("reserved", C.c_int32), ("ms_per_step", C.c_double)]
 
 
+class ModelTransform(C.Structure):
+    _fields_ = [("position", C.c_double * 3), ("rotation_deg", C.c_double * 3), ("scale", C.c_double * 3)]
+
+
+class MeshStats(C.Structure):
+    _fields_ = [("triangle_count", C.c_int64), ("vertex_count", C.c_int64), ("open_edge_count", C.c_int64),
+                ("is_watertight", C.c_int32), ("reserved", C.c_int32), ("bounding_box_size", C.c_double * 3),
+                ("characteristic_length", C.c_double), ("frontal_area", C.c_double), ("volume", C.c_double)]
+
+
 _P = C.c_void_p
 _F32P = C.POINTER(C.c_float)
 _I32P = C.POINTER(C.c_int32)
@@ -124,6 +136,13 @@ SIGNATURES = {
     "aerosim_read_wall_distance": ([_P, _F32P], C.c_int),
     "aerosim_sgs_samples": ([_P, _P, C.c_float, C.c_int32, _F32P, _F32P, _U8P], C.c_int),
     "aerosim_frontal_area": ([_F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P], C.c_int),
+    "aerosim_frontal_area_cuda": ([C.c_int32, _F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P],
+                                  C.c_int),
+    "aerosim_parse_stl": ([_U8P, C.c_int64, _F32P, C.c_int64, C.POINTER(C.c_int64), _I32P], C.c_int),
+    "aerosim_normalize_and_center": ([_F32P, C.c_int64, _I32P], C.c_int),
+    "aerosim_model_matrix": ([C.POINTER(ModelTransform), _F64P], C.c_int),
+    "aerosim_compute_mesh_stats": ([_F32P, C.c_int64, _I32P, C.c_int64, C.POINTER(ModelTransform), C.c_int32,
+                                    C.POINTER(MeshStats)], C.c_int),
     "aerosim_momentum_exchange_noalloc": ([_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, C.c_int32, _P, _P],
                                           C.c_int),
 }

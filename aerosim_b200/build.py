@@ -10,6 +10,7 @@ Translation units and their floating-point contracts:
   engine.cu     C-ABI host layer
   noalloc.cu    allocation-free force reduction entry point: -fmad=false
   sgs.cu        learned SGS closure: MLP training, wall distance, training samples
+  mesh.cu       STL reader, mesh statistics, frontal-area raster kernel: -fmad=false
 """
 from __future__ import annotations
 
@@ -40,6 +41,7 @@ UNITS = {
     "engine.cu": [],
     "noalloc.cu": ["-fmad=false"],
     "sgs.cu": [],
+    "mesh.cu": ["-fmad=false"],
 }
 
 

@@ -90,7 +90,8 @@ def lathe(points: np.ndarray, segments: int, center=(0.0, 0.0, 0.0)) -> Mesh:
 
 
 def box(sx: float, sy: float, sz: float, segments: int = 4, center=(0.0, 0.0, 0.0)) -> Mesh:
-    """Axis-aligned box with each face split into segments x segments quads."""
+    """Axis-aligned box with each face split into segments x segments quads, wound
+    counter-clockwise seen from outside."""
     pos, idx = [], []
     half = np.array([sx, sy, sz]) * 0.5
     for axis in range(3):
@@ -108,7 +109,9 @@ def box(sx: float, sy: float, sz: float, segments: int = 4, center=(0.0, 0.0, 0.
                 for i in range(segments):
                     a = base + j * (segments + 1) + i
                     b, c, d = a + 1, a + segments + 2, a + segments + 1
-                    idx += [(a, b, c), (a, c, d)] if sign > 0 else [(a, c, b), (a, d, c)]
+                    # (a, b, c) turns from u to v: outward when e_u x e_v = sign * e_axis
+                    outward = (sign > 0) != (axis == 1)
+                    idx += [(a, b, c), (a, c, d)] if outward else [(a, c, b), (a, d, c)]
     return _finish(np.array(pos) + np.asarray(center, dtype=np.float64), idx)
 
 

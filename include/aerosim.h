@@ -35,7 +35,8 @@ enum aerosim_status {
   AEROSIM_ERR_STATE = -2,     /* call out of order (e.g. step before a voxel grid) */
   AEROSIM_ERR_CUDA = -3,      /* CUDA runtime error */
   AEROSIM_ERR_DEVICE = -4,    /* a kernel reported an error status */
-  AEROSIM_ERR_NOMEM = -5      /* device allocation failed */
+  AEROSIM_ERR_NOMEM = -5,     /* device allocation failed */
+  AEROSIM_ERR_FORMAT = -6     /* malformed input file (STL) */
 };
 
 /* Cell flags, src/geometry/voxelizer.ts:12-14 */
@@ -289,6 +290,63 @@ int aerosim_batch_cells(aerosim_batch* b, int64_t* out);
 int aerosim_frontal_area(const float* positions, int64_t vertex_count, const int32_t* indices,
                          int64_t index_count, const double* world16, int32_t grid_resolution,
                          double* out);
+
+/* The same raster as a CUDA kernel on `device` (one warp per triangle, coverage bits
+ * OR'ed per pixel); returns the host raster's area bit for bit.  grid_resolution is
+ * at most 16384.  Errors: aerosim_last_error(NULL). */
+int aerosim_frontal_area_cuda(int32_t device, const float* positions, int64_t vertex_count,
+                              const int32_t* indices, int64_t index_count, const double* world16,
+                              int32_t grid_resolution, double* out);
+
+/* Formats told apart by aerosim_parse_stl. */
+enum aerosim_stl_format { AEROSIM_STL_BINARY = 0, AEROSIM_STL_ASCII = 1 };
+
+/* parseSTL(buffer), src/geometry/stlLoader.ts:9-38 (parseBinarySTL :40-75,
+ * parseAsciiSTL :77-95): the triangle soup's vertex positions, float32 xyz per vertex.
+ * With positions == NULL only *vertex_count (and *format) are set; otherwise
+ * capacity_vertices must hold *vertex_count.  The reference's exceptions ("Invalid or
+ * corrupted STL file.", "ASCII STL file contains no valid triangles.") become
+ * AEROSIM_ERR_FORMAT with that message in aerosim_last_error(NULL). */
+int aerosim_parse_stl(const uint8_t* bytes, int64_t byte_count, float* positions,
+                      int64_t capacity_vertices, int64_t* vertex_count, int32_t* format);
+
+/* normalizeAndCenterGeometry(geometry), stlLoader.ts:101-127, in place: centre the
+ * bounding box on the origin, then scale by 0.001 (largest side > 50) or to unit size
+ * (largest side in (10, 50]); *auto_scaled_from_mm (optional) is 1 when it scaled. */
+int aerosim_normalize_and_center(float* positions, int64_t vertex_count, int32_t* auto_scaled_from_mm);
+
+/* ModelTransform, src/core/types.ts:99-103 (Euler XYZ angles in degrees). */
+typedef struct {
+  double position[3];
+  double rotation_deg[3];
+  double scale[3];
+} aerosim_model_transform;
+
+/* MeshStats, src/core/types.ts:105-115 (the name stays with the caller). */
+typedef struct {
+  int64_t triangle_count;
+  int64_t vertex_count;
+  int64_t open_edge_count;
+  int32_t is_watertight;
+  int32_t reserved;
+  double bounding_box_size[3];  /* world-space size after the transform */
+  double characteristic_length; /* L_ref = max(1e-4, size x) */
+  double frontal_area;          /* A_ref, 512 x 512 raster */
+  double volume;
+} aerosim_mesh_stats;
+
+/* The world matrix computeMeshStats builds from a ModelTransform
+ * (Matrix4.compose of position, the XYZ-Euler quaternion and scale,
+ * stlLoader.ts:142-153); column-major like world16 everywhere in this header. */
+int aerosim_model_matrix(const aerosim_model_transform* transform, double* world16);
+
+/* computeMeshStats(geometry, name, transform), stlLoader.ts:133-244: welded-edge
+ * watertightness (vertices quantised to 1e-5, meshes of at most 100 000 triangles),
+ * world bounding box, L_ref, |signed volume|, and A_ref from the CUDA raster on
+ * `device` (device < 0: the host raster). */
+int aerosim_compute_mesh_stats(const float* positions, int64_t vertex_count, const int32_t* indices,
+                               int64_t index_count, const aerosim_model_transform* transform,
+                               int32_t device, aerosim_mesh_stats* out);
 
 #ifdef __cplusplus
 }
