@@ -9,6 +9,8 @@ from __future__ import annotations
 import math
 from dataclasses import dataclass
 
+from . import jsfmt
+
 # FLUID_PRESETS.air_20c, src/core/types.ts:15-22
 AIR_20C = {"id": "air_20c", "name": "Air (Sea Level, 20°C)", "density": 1.204,
            "kinematicViscosity": 1.516e-5, "speedOfSound": 343.2}
@@ -40,8 +42,8 @@ def compute_normalized_force_coefficients(fx_lat: float, fy_lat: float, fz_lat: 
 
 
 def _round_half_up(x: float, digits: int) -> float:
-    """Number(x.toFixed(digits)) for the non-negative values the tracker formats."""
-    return float(f"{x:.{digits}f}")
+    """Number(x.toFixed(digits)): ties of the exact binary value round up."""
+    return float(jsfmt.to_fixed(x, digits))
 
 
 @dataclass
