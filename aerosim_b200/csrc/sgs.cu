@@ -2,6 +2,7 @@
 // backward, Adam), its FP32 evaluation, the wall-distance field of a voxel grid (jump
 // flooding) and the training samples of a box-filtered fine-grid flow.  No counterpart
 // in the reference, whose only closure is Smagorinsky (lbmCpuReference.ts:264-282).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -11,6 +12,7 @@
 #include "common.cuh"
 #include "engine_internal.h"
 #include "sgs_mlp.cuh"
+#include "sgs_umma.cuh"
 
 namespace aerosim {
 namespace {
@@ -127,6 +129,108 @@ __global__ void mlp_forward_tc_kernel(const uint32_t* __restrict__ frag_g, const
   for (int i = 0; i < kMlpIn; ++i) x[i] = row < n ? X[row * kMlpIn + i] : 0.0f;
   const float y = mlp_nut_warp(x, frag, bias, stage[warp], lane);
   if (row < n) out[row] = y;
+}
+
+// The MLP over rows of X on the 5th-generation tensor cores: a CTA of 4 warps takes
+// 128-row tiles (grid-stride); thread t owns row t of the tile and TMEM lane t.  The
+// dynamic shared memory (kUmmaSmem) caps residency at 4 CTAs per SM, so the 4 x 128
+// allocated TMEM columns always fit.  Every mbarrier wait is bounded: on a timeout the
+// CTA records the error, waits (bounded) for its last commit and frees its TMEM.
+constexpr int kUmmaCols = 128;
+constexpr int kUmmaSmem = 56 * 1024;
+constexpr int kUmmaWaitLimit = 1 << 22;
+
+__global__ void __launch_bounds__(kUmmaRows) mlp_forward_umma_kernel(const uint4* __restrict__ bimg,
+                                                                     const float* __restrict__ bias_g,
+                                                                     const float* __restrict__ X, long long n,
+                                                                     float* __restrict__ out, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* sA1 = sm;                                          // 128 x 16 BF16
+  uint8_t* sA2 = sm + 4096;                                   // 128 x 32 BF16
+  uint8_t* sB = sm + 12288;                                   // weight image
+  float* sbias = reinterpret_cast<float*>(sm + 16384);        // [65]
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + 16384 + 512);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + 16384 + 520);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < kUmmaBBytes / 16; i += kUmmaRows) reinterpret_cast<uint4*>(sB)[i] = bimg[i];
+  for (int i = tid; i < kMlpBias; i += kUmmaRows) sbias[i] = bias_g[i];
+  *reinterpret_cast<uint4*>(sA1 + umma_off(tid, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);  // K padding
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(mbar);
+  if (tid == 0) umma_mbar_init(mb);
+  if (warp == 0) {
+    tmem_alloc((uint32_t)__cvta_generic_to_shared(tslot), kUmmaCols);
+    tmem_relinquish();
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  const uint32_t a1 = (uint32_t)__cvta_generic_to_shared(sA1), a2 = (uint32_t)__cvta_generic_to_shared(sA2),
+                 b = (uint32_t)__cvta_generic_to_shared(sB);
+  const uint64_t dA1 = umma_smem_desc(a1, 128, 256);
+  const uint64_t dA2[2] = {umma_smem_desc(a2, 128, 512), umma_smem_desc(a2 + 256, 128, 512)};
+  const uint64_t dB1 = umma_smem_desc(b + kUmmaB1, 128, 256);
+  const uint64_t dB2[2] = {umma_smem_desc(b + kUmmaB2, 128, 512), umma_smem_desc(b + kUmmaB2 + 256, 128, 512)};
+  const uint64_t dB3[2] = {umma_smem_desc(b + kUmmaB3, 128, 512), umma_smem_desc(b + kUmmaB3 + 256, 128, 512)};
+  constexpr uint32_t id32 = umma_idesc_bf16(kUmmaRows, 32), id16 = umma_idesc_bf16(kUmmaRows, 16);
+  const uint32_t lane_base = tbase + ((uint32_t)(warp * 32) << 16);
+  uint32_t phase = 0;
+  int issued = 0;  // commits issued (thread 0)
+  bool failed = false;
+  const long long tiles = (n + kUmmaRows - 1) / kUmmaRows;
+  // one layer: thread 0 issues, everyone waits; false when the CTA timed out
+  auto run = [&](auto issue) -> bool {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+      issue();
+      umma_commit(mb);
+      ++issued;
+    }
+    const bool ok = umma_mbar_wait(mb, phase, kUmmaWaitLimit);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) return false;
+    tc_fence_after();
+    return true;
+  };
+  for (long long tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
+    const long long row = tile * kUmmaRows + tid;
+    float x[kMlpIn];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) x[i] = row < n ? X[row * kMlpIn + i] : 0.0f;
+    *reinterpret_cast<uint4*>(sA1 + umma_off(tid, 0, 16)) =
+        make_uint4(bf16x2_of(x[0], x[1]), bf16x2_of(x[2], x[3]), bf16x2_of(x[4], x[5]), bf16x2_of(x[6], x[7]));
+    if (!run([&] { umma_bf16(tbase, dA1, dB1, id32, 0u); })) { failed = true; break; }
+    float d[32];
+    tmem_ld32(lane_base, d);
+    umma_store_hidden(sA2, tid, d, sbias);
+    if (!run([&] {
+          umma_bf16(tbase + 32, dA2[0], dB2[0], id32, 0u);
+          umma_bf16(tbase + 32, dA2[1], dB2[1], id32, 1u);
+        })) { failed = true; break; }
+    tmem_ld32(lane_base + 32, d);
+    umma_store_hidden(sA2, tid, d, sbias + 32);
+    if (!run([&] {
+          umma_bf16(tbase + 64, dA2[0], dB3[0], id16, 0u);
+          umma_bf16(tbase + 64, dA2[1], dB3[1], id16, 1u);
+        })) { failed = true; break; }
+    const float o = tmem_ld1(lane_base + 64) + sbias[64];
+    if (row < n) out[row] = softplus_f(o);
+    tc_fence_before();
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      umma_mbar_wait(mb, (uint32_t)((issued - 1) & 1), kUmmaWaitLimit);  // the last commit
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tbase, kUmmaCols);
 }
 
 // Adam (Kingma & Ba, 2015) on the FP32 parameters.
@@ -441,6 +545,40 @@ int aerosim_mlp_forward_tc(const float* params, const float* X, int64_t n, float
   mlp_forward_tc_kernel<<<(unsigned)((n + 127) / 128), 128>>>(F.as<uint32_t>(), B.as<float>(), Xd.as<float>(), n,
                                                               O.as<float>());
   SCU(cudaGetLastError());
+  SCU(cudaMemcpy(out, O.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+  return AEROSIM_OK;
+}
+
+int aerosim_mlp_forward_umma(const float* params, const float* X, int64_t n, float* out) {
+  if (!params || !X || !out || n < 0) return sgs_fail(AEROSIM_ERR_ARG, "mlp_forward_umma: bad argument");
+  if (n == 0) return AEROSIM_OK;
+  std::vector<uint16_t> img(kUmmaBBytes / 2);
+  std::vector<uint32_t> frag(kMlpFragWords * 32);
+  std::vector<float> bias(kMlpBias);
+  mlp_pack_umma(params, img.data());
+  mlp_pack_fragments(params, frag.data(), bias.data());
+  int dev = 0, sms = 0;
+  SCU(cudaGetDevice(&dev));
+  SCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DevBuf Bi, B, Xd, O, E;
+  SCU(Bi.alloc(kUmmaBBytes));
+  SCU(B.alloc(bias.size() * 4));
+  SCU(Xd.alloc((size_t)n * kMlpIn * 4));
+  SCU(O.alloc((size_t)n * 4));
+  SCU(E.alloc(4));
+  SCU(cudaMemcpy(Bi.p, img.data(), kUmmaBBytes, cudaMemcpyHostToDevice));
+  SCU(cudaMemcpy(B.p, bias.data(), bias.size() * 4, cudaMemcpyHostToDevice));
+  SCU(cudaMemcpy(Xd.p, X, (size_t)n * kMlpIn * 4, cudaMemcpyHostToDevice));
+  SCU(cudaMemset(E.p, 0, 4));
+  SCU(cudaFuncSetAttribute(mlp_forward_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kUmmaSmem));
+  const long long tiles = (n + kUmmaRows - 1) / kUmmaRows;
+  const unsigned grid = (unsigned)std::min<long long>(tiles, 4LL * sms);
+  mlp_forward_umma_kernel<<<grid, kUmmaRows, kUmmaSmem>>>(static_cast<const uint4*>(Bi.p), B.as<float>(),
+                                                          Xd.as<float>(), n, O.as<float>(), E.as<int>());
+  SCU(cudaGetLastError());
+  int e = 0;
+  SCU(cudaMemcpy(&e, E.p, 4, cudaMemcpyDeviceToHost));
+  if (e) return sgs_fail(AEROSIM_ERR_DEVICE, "mlp_forward_umma: tensor-core commit wait timed out");
   SCU(cudaMemcpy(out, O.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
   return AEROSIM_OK;
 }

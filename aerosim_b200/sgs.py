@@ -42,12 +42,15 @@ def _f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
-def forward(params, X, tensor_cores: bool = False) -> np.ndarray:
-    """nu_t / nu_0 for rows of X[n][8] on the GPU (FP32 CUDA cores, or the step kernel's
-    BF16 tensor-core path)."""
+def forward(params, X, tensor_cores: bool | str = False) -> np.ndarray:
+    """nu_t / nu_0 for rows of X[n][8] on the GPU: FP32 CUDA cores (False), the step
+    kernel's warp-level BF16 tensor-core path (True), or 128-row tiles on the
+    5th-generation tensor cores with accumulators in tensor memory ("tcgen05")."""
     p, x = _f32(params), _f32(X).reshape(-1, N_IN)
     out = np.empty(x.shape[0], np.float32)
-    fn = N.load().aerosim_mlp_forward_tc if tensor_cores else N.load().aerosim_mlp_forward
+    lib = N.load()
+    fn = (lib.aerosim_mlp_forward_umma if tensor_cores == "tcgen05" else
+          lib.aerosim_mlp_forward_tc if tensor_cores else lib.aerosim_mlp_forward)
     N.check(fn(N.ptr(p, C.c_float), N.ptr(x, C.c_float), x.shape[0], N.ptr(out, C.c_float)))
     return out
 

@@ -224,6 +224,10 @@ int aerosim_mlp_param_count(void);
 int aerosim_mlp_forward(const float* params, const float* X, int64_t n, float* out);
 /* The step kernel's evaluation: BF16 weights on the tensor cores, FP32 accumulation. */
 int aerosim_mlp_forward_tc(const float* params, const float* X, int64_t n, float* out);
+/* The same network on the 5th-generation tensor cores (tcgen05): 128-row tiles, BF16
+ * operands in shared memory, FP32 accumulators in tensor memory.  No reference
+ * counterpart.  AEROSIM_ERR_DEVICE when a tensor-core completion wait timed out. */
+int aerosim_mlp_forward_umma(const float* params, const float* X, int64_t n, float* out);
 /* Mean squared error against Y[n] and its gradient with respect to the parameters. */
 int aerosim_mlp_gradients(const float* params, const float* X, const float* Y, int64_t n, float* grad,
                           double* loss);

@@ -40,6 +40,21 @@ def test_forward_fp32_and_tensor_cores():
     assert np.abs(tc - ref).max() <= 0.03 * np.abs(ref).max() + 1e-3
 
 
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 70001])
+def test_forward_tcgen05_tiles(n):
+    """128-row tiles on tcgen05 (TMEM accumulators): the oracle within the BF16 bound, and
+    the warp-level tensor-core path within FP32 summation-order differences."""
+    X, _ = _data(n, 11)
+    X[::7] *= 3.0
+    p = sgs.init_params(12)
+    ref, _ = omlp.forward(p.astype(np.float64), X)
+    umma = sgs.forward(p, X, tensor_cores="tcgen05")
+    warp = sgs.forward(p, X, tensor_cores=True)
+    assert np.isfinite(umma).all()
+    assert np.abs(umma - ref).max() <= 0.03 * np.abs(ref).max() + 1e-3
+    assert np.abs(umma - warp).max() <= 1e-4 * np.abs(warp).max() + 1e-5, np.abs(umma - warp).max()
+
+
 def test_training_lowers_the_loss_and_beats_a_constant():
     X, Y = _data(20000, 4)
     p0 = sgs.init_params(5)
