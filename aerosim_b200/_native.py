@@ -130,6 +130,7 @@ SIGNATURES = {
     "aerosim_mlp_forward": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
     "aerosim_mlp_forward_tc": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
     "aerosim_mlp_forward_umma": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
+    "aerosim_mlp_last_timing": ([_F64P], C.c_int),
     "aerosim_mlp_gradients": ([_F32P, _F32P, _F32P, C.c_int64, _F32P, _F64P], C.c_int),
     "aerosim_mlp_train": ([_F32P, _F32P, _F32P, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _F32P],
                           C.c_int),

@@ -133,11 +133,12 @@ __global__ void mlp_forward_tc_kernel(const uint32_t* __restrict__ frag_g, const
 
 // The MLP over rows of X on the 5th-generation tensor cores: a CTA of 4 warps takes
 // 128-row tiles (grid-stride); thread t owns row t of the tile and TMEM lane t.  The
-// dynamic shared memory (kUmmaSmem) caps residency at 4 CTAs per SM, so the 4 x 128
-// allocated TMEM columns always fit.  Every mbarrier wait is bounded: on a timeout the
+// dynamic shared memory (kUmmaSmem) caps residency at 8 CTAs per SM, so the 8 x 64
+// allocated TMEM columns always fit: D1 in columns 0..31, D2 in 32..63, and D3 back in
+// 0..15 once D1 has been read.  Every mbarrier wait is bounded: on a timeout the
 // CTA records the error, waits (bounded) for its last commit and frees its TMEM.
-constexpr int kUmmaCols = 128;
-constexpr int kUmmaSmem = 56 * 1024;
+constexpr int kUmmaCols = 64;
+constexpr int kUmmaSmem = 27 * 1024;
 constexpr int kUmmaWaitLimit = 1 << 22;
 
 __global__ void __launch_bounds__(kUmmaRows) mlp_forward_umma_kernel(const uint4* __restrict__ bimg,
@@ -214,10 +215,10 @@ __global__ void __launch_bounds__(kUmmaRows) mlp_forward_umma_kernel(const uint4
     tmem_ld32(lane_base + 32, d);
     umma_store_hidden(sA2, tid, d, sbias + 32);
     if (!run([&] {
-          umma_bf16(tbase + 64, dA2[0], dB3[0], id16, 0u);
-          umma_bf16(tbase + 64, dA2[1], dB3[1], id16, 1u);
+          umma_bf16(tbase, dA2[0], dB3[0], id16, 0u);
+          umma_bf16(tbase, dA2[1], dB3[1], id16, 1u);
         })) { failed = true; break; }
-    const float o = tmem_ld1(lane_base + 64) + sbias[64];
+    const float o = tmem_ld1(lane_base) + sbias[64];
     if (row < n) out[row] = softplus_f(o);
     tc_fence_before();
   }
@@ -437,6 +438,30 @@ int sgs_fail(int code, const std::string& msg) {
   return code;
 }
 
+// Device time of the last forward kernel run by aerosim_mlp_forward_tc / _umma.
+double g_mlp_last_ms = 0.0;
+
+// CUDA events around one kernel launch on the default stream.
+struct KernelTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  KernelTimer() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a);
+  }
+  double stop() {
+    float ms = 0.0f;
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~KernelTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
 #define SCU(x)                                                                                       \
   do {                                                                                               \
     cudaError_t e_ = (x);                                                                            \
@@ -542,9 +567,13 @@ int aerosim_mlp_forward_tc(const float* params, const float* X, int64_t n, float
   SCU(cudaMemcpy(F.p, frag.data(), frag.size() * 4, cudaMemcpyHostToDevice));
   SCU(cudaMemcpy(B.p, bias.data(), bias.size() * 4, cudaMemcpyHostToDevice));
   SCU(cudaMemcpy(Xd.p, X, (size_t)n * kMlpIn * 4, cudaMemcpyHostToDevice));
-  mlp_forward_tc_kernel<<<(unsigned)((n + 127) / 128), 128>>>(F.as<uint32_t>(), B.as<float>(), Xd.as<float>(), n,
-                                                              O.as<float>());
-  SCU(cudaGetLastError());
+  {
+    KernelTimer t;
+    mlp_forward_tc_kernel<<<(unsigned)((n + 127) / 128), 128>>>(F.as<uint32_t>(), B.as<float>(), Xd.as<float>(), n,
+                                                                O.as<float>());
+    SCU(cudaGetLastError());
+    g_mlp_last_ms = t.stop();
+  }
   SCU(cudaMemcpy(out, O.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
   return AEROSIM_OK;
 }
@@ -572,14 +601,24 @@ int aerosim_mlp_forward_umma(const float* params, const float* X, int64_t n, flo
   SCU(cudaMemset(E.p, 0, 4));
   SCU(cudaFuncSetAttribute(mlp_forward_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kUmmaSmem));
   const long long tiles = (n + kUmmaRows - 1) / kUmmaRows;
-  const unsigned grid = (unsigned)std::min<long long>(tiles, 4LL * sms);
-  mlp_forward_umma_kernel<<<grid, kUmmaRows, kUmmaSmem>>>(static_cast<const uint4*>(Bi.p), B.as<float>(),
-                                                          Xd.as<float>(), n, O.as<float>(), E.as<int>());
-  SCU(cudaGetLastError());
+  const unsigned grid = (unsigned)std::min<long long>(tiles, 8LL * sms);
+  {
+    KernelTimer t;
+    mlp_forward_umma_kernel<<<grid, kUmmaRows, kUmmaSmem>>>(static_cast<const uint4*>(Bi.p), B.as<float>(),
+                                                            Xd.as<float>(), n, O.as<float>(), E.as<int>());
+    SCU(cudaGetLastError());
+    g_mlp_last_ms = t.stop();
+  }
   int e = 0;
   SCU(cudaMemcpy(&e, E.p, 4, cudaMemcpyDeviceToHost));
   if (e) return sgs_fail(AEROSIM_ERR_DEVICE, "mlp_forward_umma: tensor-core commit wait timed out");
   SCU(cudaMemcpy(out, O.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+  return AEROSIM_OK;
+}
+
+int aerosim_mlp_last_timing(double* ms) {
+  if (!ms) return sgs_fail(AEROSIM_ERR_ARG, "mlp_last_timing: bad argument");
+  *ms = g_mlp_last_ms;
   return AEROSIM_OK;
 }
 

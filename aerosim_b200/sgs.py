@@ -55,6 +55,13 @@ def forward(params, X, tensor_cores: bool | str = False) -> np.ndarray:
     return out
 
 
+def last_forward_ms() -> float:
+    """Device time of the kernel of the last tensor-core forward call."""
+    ms = C.c_double()
+    N.check(N.load().aerosim_mlp_last_timing(C.byref(ms)))
+    return ms.value
+
+
 def gradients(params, X, Y) -> tuple[np.ndarray, float]:
     """(gradient, loss) of the mean squared error on the GPU."""
     p, x, y = _f32(params), _f32(X).reshape(-1, N_IN), _f32(Y).ravel()

@@ -242,7 +242,8 @@ def run_ours(args) -> dict:
             "nan": nan, "inference": "BF16 mma.sync m16n8k16 tiles, FP32 accumulation, inside the step kernel",
             "training": {k: meta[k] for k in ("fine", "coarse", "fine_cd_mean", "heldout_mse_mlp",
                                                "heldout_mse_smagorinsky", "coarse_smagorinsky", "coarse_mlp")
-                         if k in meta}}
+                         if k in meta},
+            "forward_tiles": closure_forward_tiles(w["params"], cells)}
 
     # ---- batched sweep: 32 wings of uneven lattice sizes, one launch per step ----
     if args.batch_steps > 0:
@@ -332,6 +333,23 @@ def run_ours(args) -> dict:
                    "parallelism": f"{ws} independent lattices, one per GPU (weak scaling)"},
     })
     return out if rank == 0 else {}
+
+
+def closure_forward_tiles(params, rows: int, reps: int = 3) -> dict:
+    """The closure network over one lattice's worth of cells (seeded inputs) on both
+    tensor-core paths: 128-row tcgen05 tiles with TMEM accumulators, and the step
+    kernel's warp-level mma.sync evaluation; device time of the kernel, best of reps."""
+    from aerosim_b200 import sgs
+    X = np.random.default_rng(0).normal(0.0, 1.0, (rows, 8)).astype(np.float32)
+    res = {"rows": rows, "flops_per_row": 4096, "note": "flops of the padded tiles (K 16 / 32, N 32 / 32 / 16)"}
+    for key, tc in (("tcgen05", "tcgen05"), ("mma_sync", True)):
+        best = float("inf")
+        for _ in range(reps):
+            sgs.forward(params, X, tensor_cores=tc)
+            best = min(best, sgs.last_forward_ms())
+        res[key] = {"ms": round(best, 4), "rows_per_s": round(rows / (best * 1e-3), 1),
+                    "tflops": round(rows * 4096 / (best * 1e-3) / 1e12, 3)}
+    return res
 
 
 def run_batch(args, dev: int, ws: int, barrier_sync, max_over_ranks) -> dict:

@@ -228,6 +228,9 @@ int aerosim_mlp_forward_tc(const float* params, const float* X, int64_t n, float
  * operands in shared memory, FP32 accumulators in tensor memory.  No reference
  * counterpart.  AEROSIM_ERR_DEVICE when a tensor-core completion wait timed out. */
 int aerosim_mlp_forward_umma(const float* params, const float* X, int64_t n, float* out);
+/* Device time (CUDA events) of the kernel of the last aerosim_mlp_forward_tc /
+ * aerosim_mlp_forward_umma call in this process. */
+int aerosim_mlp_last_timing(double* ms);
 /* Mean squared error against Y[n] and its gradient with respect to the parameters. */
 int aerosim_mlp_gradients(const float* params, const float* X, const float* Y, int64_t n, float* grad,
                           double* loss);
