@@ -113,6 +113,8 @@ SIGNATURES = {
     "aerosim_write_populations": ([_P, _P, C.c_int32], C.c_int),
     "aerosim_extract_slice": ([_P, C.c_int32, C.c_double, C.c_int32, _U8P, C.POINTER(C.c_int32),
                                C.POINTER(C.c_int32)], C.c_int),
+    "aerosim_step_and_extract_slice": ([_P, C.c_int32, C.c_int32, C.c_double, C.c_int32, _U8P, _I32P, _I32P,
+                                        C.POINTER(Forces)], C.c_int),
     "aerosim_q_criterion": ([_P, _F32P, _F32P, _F32P, _F64P, _F64P], C.c_int),
     "aerosim_q_criterion_fields": ([_P, C.c_int32, C.c_int32, C.c_int32, C.c_double, _F32P, _F32P, _F32P, _U8P,
                                     _F32P, _F32P, _F32P, _F64P, _F64P], C.c_int),

@@ -56,6 +56,7 @@ struct aerosim_engine {
   unsigned long long* stats_buf = nullptr;
   void* staging = nullptr;
   size_t staging_bytes = 0;
+  double* frame_host = nullptr;  // pinned: force sums [8] and the device error flag of a frame
   long long step_index = 0;
   double last_ms = 0;
   long long last_launches = 0;
@@ -430,6 +431,7 @@ int aerosim_destroy(aerosim_engine* h) {
   cudaFree(h->near_cells); cudaFree(h->links);
   cudaFree(h->force_partials); cudaFree(h->force_ticket); cudaFree(h->force_out);
   cudaFree(h->stats_buf); cudaFree(h->staging);
+  if (h->frame_host) cudaFreeHost(h->frame_host);
   cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -594,8 +596,13 @@ int aerosim_reset_flow(aerosim_engine* h) {
   return do_reset(h);
 }
 
-int aerosim_step(aerosim_engine* h, int32_t n) {
-  if (!h) return AEROSIM_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// Enqueues n steps on h's stream between the engine's timing events (the substep loop
+// of stepAndExtractSlice, lbmEngine.ts:483-527); the caller synchronizes.
+int enqueue_steps(aerosim_engine* h, int32_t n) {
   if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "step: no voxel grid");
   if (n < 0) return fail(h, AEROSIM_ERR_ARG, "step: negative step count");
   if (h->step_index + n > 0x7fffffffLL) return fail(h, AEROSIM_ERR_ARG, "step: step index overflow");
@@ -631,15 +638,55 @@ int aerosim_step(aerosim_engine* h, int32_t n) {
     h->step_index += 1;
   }
   CU(h, cudaEventRecord(h->ev1, h->stream));
-  int dev_err = 0;
-  CU(h, cudaMemcpyAsync(&dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  CU(h, cudaStreamSynchronize(h->stream));
+  h->last_launches = launches;
+  return AEROSIM_OK;
+}
+
+// Step timing after the stream has drained.
+int finish_steps(aerosim_engine* h, int dev_err) {
   float ms = 0.f;
   CU(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->last_ms = ms;
-  h->last_launches = launches;
   if (dev_err) return fail(h, AEROSIM_ERR_DEVICE, "step: the shared-memory pipeline timed out (device error flag set)");
   return AEROSIM_OK;
+}
+
+// Enqueues the momentum-exchange reduction of the current populations; its eight FP64
+// sums land in `dst` (device-to-host, asynchronous when dst is pinned).
+int enqueue_forces(aerosim_engine* h, double* dst) {
+  ForceArgs a{};
+  a.f = h->f[h->cur];
+  a.cls = h->g.cls; a.bcells = h->g.bcells; a.q = h->g.q; a.st = h->st;
+  a.partials = h->force_partials; a.ticket = h->force_ticket; a.out = h->force_out;
+  a.L = h->L; a.B = h->g.B;
+  a.prev_slot = prev_slot(h);
+  const unsigned grid = (unsigned)std::min<long long>((h->g.B + 7) / 8, h->force_blocks_cap);
+  CU(h, launch_forces(h->cfg.precision, a, grid, h->stream));
+  CU(h, cudaMemcpyAsync(dst, h->force_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return AEROSIM_OK;
+}
+
+void forces_from_sums(aerosim_engine* h, const double* r, aerosim_forces* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->fx = r[0]; out->fy = r[1]; out->fz = r[2];
+  out->mx = r[3]; out->my = r[4]; out->mz = r[5];
+  out->cut_face_links = (int64_t)r[6];
+  out->step = h->step_index;
+  coefficients(h->cfg, h->dx, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+int aerosim_step(aerosim_engine* h, int32_t n) {
+  if (!h) return AEROSIM_ERR_ARG;
+  int rc = enqueue_steps(h, n);
+  if (rc) return rc;
+  int dev_err = 0;
+  CU(h, cudaMemcpyAsync(&dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaStreamSynchronize(h->stream));
+  return finish_steps(h, dev_err);
 }
 
 int aerosim_get_step_count(aerosim_engine* h, int64_t* out) {
@@ -654,23 +701,11 @@ int aerosim_read_forces(aerosim_engine* h, aerosim_forces* out) {
   CU(h, cudaSetDevice(h->device));
   double r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (h->g.B > 0) {
-    ForceArgs a{};
-    a.f = h->f[h->cur];
-    a.cls = h->g.cls; a.bcells = h->g.bcells; a.q = h->g.q; a.st = h->st;
-    a.partials = h->force_partials; a.ticket = h->force_ticket; a.out = h->force_out;
-    a.L = h->L; a.B = h->g.B;
-    a.prev_slot = prev_slot(h);
-    const unsigned grid = (unsigned)std::min<long long>((h->g.B + 7) / 8, h->force_blocks_cap);
-    CU(h, launch_forces(h->cfg.precision, a, grid, h->stream));
-    CU(h, cudaMemcpyAsync(r, h->force_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    int rc = enqueue_forces(h, r);
+    if (rc) return rc;
     CU(h, cudaStreamSynchronize(h->stream));
   }
-  std::memset(out, 0, sizeof(*out));
-  out->fx = r[0]; out->fy = r[1]; out->fz = r[2];
-  out->mx = r[3]; out->my = r[4]; out->mz = r[5];
-  out->cut_face_links = (int64_t)r[6];
-  out->step = h->step_index;
-  coefficients(h->cfg, h->dx, out);
+  forces_from_sums(h, r, out);
   return AEROSIM_OK;
 }
 
@@ -835,9 +870,11 @@ int aerosim_frontal_area(const float* pos, int64_t nv, const int32_t* idx, int64
 
 }  // extern "C"
 
-extern "C" int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fraction, int32_t mode, uint8_t* rgba,
-                                     int32_t* width, int32_t* height) {
-  if (!h || !width || !height) return AEROSIM_ERR_ARG;
+namespace {
+
+// Slice size and, with rgba, the enqueued slice kernel and its copy to rgba.
+int enqueue_slice(aerosim_engine* h, int32_t axis, double fraction, int32_t mode, uint8_t* rgba, int32_t* width,
+                  int32_t* height) {
   if (axis < 0 || axis > 2 || mode < 0 || mode > 2) return fail(h, AEROSIM_ERR_ARG, "extract_slice: bad axis or mode");
   if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "extract_slice: no voxel grid");
   const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz;
@@ -857,7 +894,43 @@ extern "C" int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fra
   CU(h, launch_slice(h->mux, h->muy, h->muz, h->mrho, h->g.cls, h->st, prev_slot(h), h->L, axis, fixed, mode,
                      js_max(1e-4, h->cfg.u_inlet_lattice), w, hh, static_cast<uint8_t*>(h->staging), h->stream));
   CU(h, cudaMemcpyAsync(rgba, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+  return AEROSIM_OK;
+}
+
+}  // namespace
+
+extern "C" int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fraction, int32_t mode, uint8_t* rgba,
+                                     int32_t* width, int32_t* height) {
+  if (!h || !width || !height) return AEROSIM_ERR_ARG;
+  int rc = enqueue_slice(h, axis, fraction, mode, rgba, width, height);
+  if (rc || !rgba) return rc;
   CU(h, cudaStreamSynchronize(h->stream));
+  return AEROSIM_OK;
+}
+
+// stepAndExtractSlice(substeps), lbmEngine.ts:404-675, as one call: the substeps, the
+// force reduction and (with rgba) the slice image are enqueued back to back and the
+// stream is drained once; the force sums and the device error flag return through a
+// pinned buffer of the engine.
+extern "C" int aerosim_step_and_extract_slice(aerosim_engine* h, int32_t n, int32_t axis, double fraction,
+                                              int32_t mode, uint8_t* rgba, int32_t* width, int32_t* height,
+                                              aerosim_forces* forces) {
+  if (!h || !forces || (rgba && (!width || !height))) return AEROSIM_ERR_ARG;
+  if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "step_and_extract_slice: no voxel grid");
+  CU(h, cudaSetDevice(h->device));
+  if (!h->frame_host) CU(h, cudaHostAlloc((void**)&h->frame_host, 16 * sizeof(double), cudaHostAllocDefault));
+  double* sums = h->frame_host;
+  int* dev_err = reinterpret_cast<int*>(h->frame_host + 8);
+  *dev_err = 0;
+  for (int i = 0; i < 8; ++i) sums[i] = 0.0;
+  int rc = enqueue_steps(h, n);
+  if (rc) return rc;
+  CU(h, cudaMemcpyAsync(dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (h->g.B > 0 && (rc = enqueue_forces(h, sums))) return rc;
+  if (rgba && (rc = enqueue_slice(h, axis, fraction, mode, rgba, width, height))) return rc;
+  CU(h, cudaStreamSynchronize(h->stream));
+  if ((rc = finish_steps(h, *dev_err))) return rc;
+  forces_from_sums(h, sums, forces);
   return AEROSIM_OK;
 }
 

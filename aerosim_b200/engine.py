@@ -301,15 +301,24 @@ class LBMEngine:
         'fraction', 'mode'}) also the slice image (width, height, rgba)."""
         if not self._has_grid:
             return None
-        self.step(substeps)
-        f = self.read_forces()
+        f = N.Forces()
+        w, h = C.c_int32(), C.c_int32()
+        if slice is None:
+            self._h.call("aerosim_step_and_extract_slice", int(substeps), 2, 0.5, 0, None, None, None, C.byref(f))
+        else:
+            a = {"x": 0, "y": 1, "z": 2}[slice.get("axis", "z")]
+            m = {"velocity": 0, "vorticity": 1, "pressure": 2}[slice.get("mode", "velocity")]
+            frac = float(slice.get("fraction", 0.5))
+            self._h.call("aerosim_extract_slice", a, frac, m, None, C.byref(w), C.byref(h))
+            rgba = np.empty(w.value * h.value * 4, np.uint8)
+            self._h.call("aerosim_step_and_extract_slice", int(substeps), a, frac, m, N.ptr(rgba, C.c_uint8),
+                         C.byref(w), C.byref(h), C.byref(f))
         c = self.config
         readout = self.force_tracker.push_sample(f.step, f.cd, f.cl, f.cm, f.xcp, c["windSpeedMps"],
                                                  c["fluid"], c["frontalAreaM2"])
         out = {"stepCount": int(f.step), "forceReadout": readout, "forces": f}
         if slice is not None:
-            out.update(self.extract_slice_rgba(slice.get("axis", "z"), slice.get("fraction", 0.5),
-                                               slice.get("mode", "velocity")))
+            out.update({"width": w.value, "height": h.value, "rgba": rgba})
         if read_macro_field:
             out["macroField"] = self.read_macro()
         return out

@@ -197,8 +197,8 @@ def run_ours(args) -> dict:
         frame_d2h = ctypes.sizeof(N.Forces) + 4 + fr["rgba"].nbytes
         out["e2e"] = {"value": round(ws * cells * 4 * frames / dt / 1e6, 1), "unit": "MLUPS",
                       "h2d_bytes_per_step": 0, "d2h_bytes_per_step": frame_d2h // 4,
-                      "frame": "stepAndExtractSlice: aerosim_step(4 substeps) + aerosim_read_forces (FP64 sums) "
-                               "+ aerosim_extract_slice (z = nz/2 velocity RGBA), results copied to the host",
+                      "frame": "stepAndExtractSlice: aerosim_step_and_extract_slice (4 substeps, FP64 force sums, "
+                               "z = nz/2 velocity RGBA slice, one synchronization), results copied to the host",
                       "frames": frames}
     eng.close()
 

@@ -171,6 +171,11 @@ int aerosim_mass_stats(aerosim_engine* h, aerosim_mass* out);
  * width * height * 4 bytes, row v at v * width * 4; NULL only reports the size. */
 int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fraction, int32_t mode, uint8_t* rgba,
                           int32_t* width, int32_t* height);
+/* stepAndExtractSlice(substeps), lbmEngine.ts:404-675, as one call: n substeps, the
+ * force readout (as aerosim_read_forces) and, when rgba is not NULL, the slice image
+ * (as aerosim_extract_slice), with one synchronization instead of three. */
+int aerosim_step_and_extract_slice(aerosim_engine* h, int32_t n, int32_t axis, double fraction, int32_t mode,
+                                   uint8_t* rgba, int32_t* width, int32_t* height, aerosim_forces* forces);
 
 /* ---- timing support -------------------------------------------------------- */
 

@@ -298,3 +298,25 @@ def test_slice_images_match_the_oracle(gpu_engine_cls, oracle_mod, precision):
                 assert diff.max() == 0, (axis, mode)
             else:
                 assert diff.max() <= 2 and np.mean(diff > 0) < 0.01, (axis, mode, diff.max())
+
+
+def test_fused_frame_equals_separate_calls(gpu_engine_cls, oracle_mod):
+    """aerosim_step_and_extract_slice (one synchronization) gives the same force sums,
+    coefficients and slice bytes as aerosim_step + aerosim_read_forces +
+    aerosim_extract_slice on a twin engine, frame after frame, with and without a slice."""
+    case = cases.sphere_64x32x32()
+    _, _, fused = _pair(gpu_engine_cls, oracle_mod, case, "f32")
+    _, _, split = _pair(gpu_engine_cls, oracle_mod, case, "f32")
+    sl = {"axis": "y", "fraction": 0.5, "mode": "vorticity"}
+    for k in range(4):
+        a = fused.step_and_extract_slice(4, slice=sl if k % 2 == 0 else None)
+        split.step(4)
+        fb = split.read_forces()
+        fa = a["forces"]
+        assert (fa.fx, fa.fy, fa.fz, fa.mz, fa.cd, fa.cl, fa.step) == (fb.fx, fb.fy, fb.fz, fb.mz, fb.cd, fb.cl, fb.step)
+        if k % 2 == 0:
+            b = split.extract_slice_rgba("y", 0.5, "vorticity")
+            assert (a["width"], a["height"]) == (b["width"], b["height"])
+            assert np.array_equal(a["rgba"], b["rgba"])
+    fused.close()
+    split.close()
