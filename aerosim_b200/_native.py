@@ -71,7 +71,7 @@ class Mass(C.Structure):
 
 class BatchTuning(C.Structure):
     _fields_ = [("stages", C.c_int32), ("ctas_per_sm", C.c_int32), ("graph_steps", C.c_int32),
-                ("reserved", C.c_int32), ("ms_per_step", C.c_double)]
+                ("item_cells", C.c_int32), ("ms_per_step", C.c_double)]
 
 
 class ModelTransform(C.Structure):

@@ -57,6 +57,7 @@ struct aerosim_engine {
   void* staging = nullptr;
   size_t staging_bytes = 0;
   double* frame_host = nullptr;  // pinned: force sums [8] and the device error flag of a frame
+  aerosim_batch* solo = nullptr;  // 16-bit storage: this lattice as a batch of one (see solo_enqueue)
   long long step_index = 0;
   double last_ms = 0;
   long long last_launches = 0;
@@ -67,6 +68,10 @@ struct aerosim_engine {
 };
 
 namespace {
+
+void solo_release(aerosim_engine* h);
+int solo_enqueue(aerosim_engine* h, int32_t n, long long* launches);
+bool solo_eligible(const aerosim_engine* h);
 
 std::string g_create_error;
 std::mutex g_error_mu;
@@ -96,6 +101,7 @@ void free_grid(DevGrid& g) {
 }
 
 void free_pops(aerosim_engine* h) {
+  solo_release(h);
   cudaFree(h->f[0]); cudaFree(h->f[1]);
   h->f[0] = h->f[1] = nullptr;
   cudaFree(h->mux); cudaFree(h->muy); cudaFree(h->muz); cudaFree(h->mrho);
@@ -225,6 +231,7 @@ int upload_tables(aerosim_engine* h) {
 
 // Installs a freshly built device grid (voxelizer output or host upload).
 int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[3], int reset_flow) {
+  solo_release(h);  // its near-wall list and item table belong to the previous grid
   // A pending rescale belongs to the old flags: apply it before they change.
   if (h->have_grid && h->f[0] && !reset_flow) {
     CU(h, launch_materialize(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->L, h->g.N,
@@ -425,6 +432,7 @@ int aerosim_destroy(aerosim_engine* h) {
   if (!h) return AEROSIM_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  solo_release(h);
   free_grid(h->g);
   free_pops(h);
   cudaFree(h->abl); cudaFree(h->sin_tab); cudaFree(h->st);
@@ -626,21 +634,29 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.mlp_nu0 = (float)((std::max(a.tau0, 0.5015) - 0.5) / 3.0);
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
-  for (int s = 0; s < n; ++s) {
-    a.fsrc = h->f[h->cur];
-    a.fdst = h->f[h->cur ^ 1];
-    a.step_index = (int)h->step_index;
-    a.write_macro = (s == n - 1) ? 1 : 0;
-    int nl = 0;
-    CU(h, launch_step(h->cfg.precision, a, h->block, h->grid, h->smem, h->stream, nullptr, &nl));
-    launches += nl;
-    h->cur ^= 1;
-    h->step_index += 1;
+  if (solo_eligible(h)) {
+    int rc = solo_enqueue(h, n, &launches);
+    if (rc) return rc;
+  } else {
+    for (int s = 0; s < n; ++s) {
+      a.fsrc = h->f[h->cur];
+      a.fdst = h->f[h->cur ^ 1];
+      a.step_index = (int)h->step_index;
+      a.write_macro = (s == n - 1) ? 1 : 0;
+      int nl = 0;
+      CU(h, launch_step(h->cfg.precision, a, h->block, h->grid, h->smem, h->stream, nullptr, &nl));
+      launches += nl;
+      h->cur ^= 1;
+      h->step_index += 1;
+    }
   }
   CU(h, cudaEventRecord(h->ev1, h->stream));
   h->last_launches = launches;
   return AEROSIM_OK;
 }
+
+// The device flag a step path raises when its shared-memory pipeline timed out.
+int* step_error_flag(aerosim_engine* h);
 
 // Step timing after the stream has drained.
 int finish_steps(aerosim_engine* h, int dev_err) {
@@ -684,7 +700,7 @@ int aerosim_step(aerosim_engine* h, int32_t n) {
   int rc = enqueue_steps(h, n);
   if (rc) return rc;
   int dev_err = 0;
-  CU(h, cudaMemcpyAsync(&dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaMemcpyAsync(&dev_err, step_error_flag(h), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(h, cudaStreamSynchronize(h->stream));
   return finish_steps(h, dev_err);
 }
@@ -925,7 +941,7 @@ extern "C" int aerosim_step_and_extract_slice(aerosim_engine* h, int32_t n, int3
   for (int i = 0; i < 8; ++i) sums[i] = 0.0;
   int rc = enqueue_steps(h, n);
   if (rc) return rc;
-  CU(h, cudaMemcpyAsync(dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaMemcpyAsync(dev_err, step_error_flag(h), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (h->g.B > 0 && (rc = enqueue_forces(h, sums))) return rc;
   if (rgba && (rc = enqueue_slice(h, axis, fraction, mode, rgba, width, height))) return rc;
   CU(h, cudaStreamSynchronize(h->stream));
@@ -1021,6 +1037,8 @@ extern "C" {
 int aerosim_set_sgs_mlp(aerosim_engine* h, const float* params) {
   if (!h) return AEROSIM_ERR_ARG;
   CU(h, cudaSetDevice(h->device));
+  CU(h, cudaStreamSynchronize(h->stream));
+  solo_release(h);  // the closure runs in main_kernel
   if (!params) {
     cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
     h->mlp_frag = nullptr;
@@ -1117,6 +1135,7 @@ struct aerosim_batch {
   int* d_error = nullptr;
   long long n_items = 0, n_near = 0, cells = 0;
   long long slot_elems = 0, slot_cls = 0;
+  int item_cells = 0;  // cells per work item of the current item list
   int pitch = 0;  // row pitch shared by all instances (0: they differ)
   int num_sms = 148;
   aerosim_batch_tuning tune{};
@@ -1125,6 +1144,7 @@ struct aerosim_batch {
   cudaGraphExec_t graph = nullptr;
   int graph_len = 0;
   int step = 0;
+  bool own_stream = true;  // false for an engine's batch of one, which runs on the engine's stream
   double last_ms = 0;
   long long last_launches = 0;
 };
@@ -1148,7 +1168,7 @@ void batch_free(aerosim_batch* b) {
   cudaFree(b->d_partials); cudaFree(b->d_ticket); cudaFree(b->d_step); cudaFree(b->d_error);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
-  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
 }
 
 // The solver arguments of every instance, from its engine's current configuration.
@@ -1184,9 +1204,47 @@ BatchArgs batch_args(const aerosim_batch* b, int write_macro) {
 
 // Launch shape of a tuning: the shared memory of its ring and the persistent grid, or
 // an error when the configuration does not fit.
+// Rows per work item of a lattice for a target of item_cells cells per item (0: 256).
+int batch_rows_per_item(const Layout& L, int item_cells) {
+  const int span = (L.nx + row_shift(L.nx) + 31) / 32 * 32;
+  if (item_cells <= 0) return rows_per_item(L.nx);
+  return std::max(1, std::min(kMaxRowsPerItem, item_cells / span));
+}
+
+// The flat item list for item_cells cells per item: first item of each instance, rows per
+// item / segments per row / row shift of each instance, and the ring slot sizes.
+int batch_build_items(aerosim_batch* b, int item_cells) {
+  const int n = (int)b->eng.size();
+  std::vector<long long> item_begin(n + 1, 0);
+  std::vector<int4> geo(n);
+  long long slot_elems = 0, slot_cls = 0;
+  for (int k = 0; k < n; ++k) {
+    const Layout& L = b->eng[k]->L;
+    const int RY = batch_rows_per_item(L, item_cells);
+    const long long rows = (long long)L.ny * L.nz;
+    item_begin[k + 1] = item_begin[k] + (rows + RY - 1) / RY;
+    geo[k] = make_int4(RY, (L.nx + row_shift(L.nx) + 31) / 32, row_shift(L.nx), 0);
+    slot_elems = std::max<long long>(slot_elems, (long long)RY * 19 * L.pitch);
+    slot_cls = std::max<long long>(slot_cls, (long long)RY * L.pitch);
+  }
+  BCU(cudaMemcpy(b->d_item_begin, item_begin.data(), item_begin.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  BCU(cudaMemcpy(b->d_geo, geo.data(), geo.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  b->n_items = item_begin[n];
+  b->slot_elems = slot_elems;
+  b->slot_cls = slot_cls;
+  b->item_cells = item_cells;
+  return AEROSIM_OK;
+}
+
 int batch_configure(aerosim_batch* b, const aerosim_batch_tuning& t, unsigned* grid, size_t* smem) {
-  if (t.stages < 2 || t.stages > 6 || t.ctas_per_sm < 1 || t.ctas_per_sm > 3 || t.graph_steps < 1)
-    return bfail(AEROSIM_ERR_ARG, "batch: tuning out of range (stages 2..6, ctas_per_sm 1..3, graph_steps >= 1)");
+  if (t.stages < 2 || t.stages > 6 || t.ctas_per_sm < 1 || t.ctas_per_sm > 3 || t.graph_steps < 1 ||
+      t.item_cells < 0 || t.item_cells > 2048)
+    return bfail(AEROSIM_ERR_ARG,
+                 "batch: tuning out of range (stages 2..6, ctas_per_sm 1..3, graph_steps >= 1, item_cells 0..2048)");
+  if (t.item_cells != b->item_cells) {
+    int rc = batch_build_items(b, t.item_cells);
+    if (rc) return rc;
+  }
   const size_t eb = precision_bytes(b->precision);
   const size_t sm = batch_smem_bytes(b->slot_elems, b->slot_cls, t.stages, eb);
   if (sm > 227 * 1024) return bfail(AEROSIM_ERR_ARG, "batch: the ring does not fit shared memory");
@@ -1205,8 +1263,16 @@ int batch_configure(aerosim_batch* b, const aerosim_batch_tuning& t, unsigned* g
 int batch_apply_tuning(aerosim_batch* b, const aerosim_batch_tuning& t) {
   unsigned grid = 0;
   size_t smem = 0;
+  const int prev_cells = b->item_cells;
   int rc = batch_configure(b, t, &grid, &smem);
-  if (rc) return rc;
+  if (rc) {
+    // keep the item list of the configuration in force
+    if (b->item_cells != prev_cells) {
+      std::string msg = aerosim_last_error(nullptr);
+      if (batch_build_items(b, prev_cells) == AEROSIM_OK) bfail(rc, msg);
+    }
+    return rc;
+  }
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -1273,6 +1339,99 @@ int batch_enqueue(aerosim_batch* b, int n, long long* launches) {
   return AEROSIM_OK;
 }
 
+// ---- 16-bit storage: the lattice as a batch of one ----------------------------------
+// Engines with FP16S or BF16S storage and no learned closure step through the batched
+// kernel with work items of 1024 cells (4 x-rows of 256): at 256x128x128 that takes
+// 94.9 us per step against 102.4 us for main_kernel, whose work items are single rows
+// (the per-item pipeline round trips are amortised over four times the cells).  The
+// batch runs on the engine's own stream and reads the engine's state; it is rebuilt
+// when the engine's buffers or grid change, and it never resets the flow.
+
+bool solo_eligible(const aerosim_engine* h) {
+  return (h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S) && !h->mlp_frag;
+}
+
+void solo_release(aerosim_engine* h) {
+  if (!h->solo) return;
+  batch_free(h->solo);
+  delete h->solo;
+  h->solo = nullptr;
+}
+
+int* step_error_flag(aerosim_engine* h) { return h->solo && solo_eligible(h) ? h->solo->d_error : &h->st->error; }
+
+int solo_create(aerosim_engine* h) {
+  aerosim_batch* b = new (std::nothrow) aerosim_batch();
+  if (!b) return fail(h, AEROSIM_ERR_NOMEM, "step: out of host memory");
+  b->device = h->device;
+  b->precision = h->cfg.precision;
+  b->eng.assign(1, h);
+  b->num_sms = h->num_sms;
+  b->stream = h->stream;
+  b->own_stream = false;
+  b->cells = h->g.N;
+  b->n_near = h->n_near;
+  const int p = h->L.pitch;
+  b->pitch = (p == 64 || p == 128 || p == 192 || p == 256) ? p : 0;
+  b->step = -1;  // the device step counter is written before the first launch
+  h->solo = b;
+  void* bufs[2] = {h->f[0], h->f[1]};
+  const long long near_begin[2] = {0, h->n_near};
+  CU(h, cudaEventCreate(&b->ev0));
+  CU(h, cudaEventCreate(&b->ev1));
+  CU(h, cudaMalloc(&b->d_inst, sizeof(StepArgs)));
+  CU(h, cudaMalloc(&b->d_bufs, 2 * sizeof(void*)));
+  CU(h, cudaMalloc(&b->d_item_begin, 2 * sizeof(long long)));
+  CU(h, cudaMalloc(&b->d_near_begin, 2 * sizeof(long long)));
+  CU(h, cudaMalloc(&b->d_geo, sizeof(int4)));
+  CU(h, cudaMalloc(&b->d_partials, (size_t)3 * b->num_sms * sizeof(unsigned long long)));
+  CU(h, cudaMalloc(&b->d_ticket, 2 * sizeof(unsigned int)));
+  CU(h, cudaMalloc(&b->d_step, sizeof(int)));
+  CU(h, cudaMalloc(&b->d_error, sizeof(int)));
+  CU(h, cudaMemcpy(b->d_bufs, bufs, sizeof(bufs), cudaMemcpyHostToDevice));
+  CU(h, cudaMemcpy(b->d_near_begin, near_begin, sizeof(near_begin), cudaMemcpyHostToDevice));
+  CU(h, cudaMemset(b->d_error, 0, sizeof(int)));
+  // the first configuration that fits: 1024-cell items, then smaller ones
+  static const aerosim_batch_tuning kTry[] = {{2, 2, 20, 1024, 0.0}, {3, 2, 20, 1024, 0.0}, {2, 1, 20, 1024, 0.0},
+                                              {2, 2, 20, 512, 0.0},  {3, 3, 20, 0, 0.0},    {2, 1, 20, 0, 0.0}};
+  int rc = AEROSIM_ERR_ARG;
+  for (const aerosim_batch_tuning& t : kTry)
+    if ((rc = batch_apply_tuning(b, t)) == AEROSIM_OK) break;
+  if (rc) return fail(h, rc, std::string("step: no batched launch fits: ") + aerosim_last_error(nullptr));
+  return AEROSIM_OK;
+}
+
+// Enqueues n steps of the batch of one on the engine's stream and advances the
+// engine's step count and buffer parity.
+int solo_enqueue(aerosim_engine* h, int32_t n, long long* launches) {
+  if (!h->solo) {
+    int rc = solo_create(h);
+    if (rc) {
+      solo_release(h);
+      return rc;
+    }
+  }
+  aerosim_batch* b = h->solo;
+  if (b->step != h->step_index) {
+    // first launch, or main_kernel / a reset moved the step count: restart the counter
+    // and the CTA tickets at the engine's step
+    const int s0 = (int)h->step_index;
+    CU(h, cudaMemcpyAsync(b->d_step, &s0, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CU(h, cudaMemsetAsync(b->d_ticket, 0, 2 * sizeof(unsigned int), h->stream));
+    b->step = s0;
+  }
+  int rc = batch_upload_table(b);
+  if (!rc) rc = batch_enqueue(b, n, launches);
+  if (rc) return fail(h, rc, aerosim_last_error(nullptr));
+  b->step += n;
+  h->step_index += n;
+  h->cur = (int)(h->step_index & 1);
+  // main_kernel's density accumulators (rho_sum[2], ticket[2]) start from zero whenever
+  // it takes over again
+  CU(h, cudaMemsetAsync(h->st, 0, 2 * sizeof(unsigned long long) + 2 * sizeof(unsigned int), h->stream));
+  return AEROSIM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1307,27 +1466,19 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
     return bfail(rc, msg);
   };
   cudaError_t e = cudaSetDevice(b->device);
-  std::vector<long long> item_begin(n + 1, 0), near_begin(n + 1, 0);
+  std::vector<long long> near_begin(n + 1, 0);
   std::vector<void*> bufs(2 * (size_t)n);
-  std::vector<int4> geo(n);
   int pitch = engines[0]->L.pitch;
   for (int k = 0; k < n; ++k) {
     const aerosim_engine* en = engines[k];
     const Layout& L = en->L;
-    const int RY = rows_per_item(L.nx);
-    const long long rows = (long long)L.ny * L.nz;
-    item_begin[k + 1] = item_begin[k] + (rows + RY - 1) / RY;
     near_begin[k + 1] = near_begin[k] + en->n_near;
-    geo[k] = make_int4(RY, (L.nx + row_shift(L.nx) + 31) / 32, row_shift(L.nx), 0);
     bufs[2 * k] = en->f[0];
     bufs[2 * k + 1] = en->f[1];
-    b->slot_elems = std::max<long long>(b->slot_elems, (long long)RY * 19 * L.pitch);
-    b->slot_cls = std::max<long long>(b->slot_cls, (long long)RY * L.pitch);
     b->cells += en->g.N;
     if (L.pitch != pitch) pitch = 0;
   }
   b->pitch = (pitch == 64 || pitch == 128 || pitch == 192 || pitch == 256) ? pitch : 0;
-  b->n_items = item_begin[n];
   b->n_near = near_begin[n];
   const size_t part = (size_t)3 * b->num_sms * n;
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
@@ -1345,15 +1496,14 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_bufs, bufs.data(), bufs.size() * sizeof(void*), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_item_begin, item_begin.data(), item_begin.size() * sizeof(long long), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
     e = cudaMemcpy(b->d_near_begin, near_begin.data(), near_begin.size() * sizeof(long long), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_geo, geo.data(), geo.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     bfail(AEROSIM_ERR_CUDA, std::string("batch_create: ") + cudaGetErrorString(e));
     return bail(AEROSIM_ERR_CUDA);
   }
-  int rc = batch_reset(b);
+  int rc = batch_build_items(b, 0);
+  if (rc) return bail(rc);
+  rc = batch_reset(b);
   if (!rc) rc = batch_upload_table(b);
   if (rc) return bail(rc);
   // default launch: the most resident CTAs per SM that a 3-slot ring allows (at least a
@@ -1414,19 +1564,20 @@ int aerosim_batch_autotune(aerosim_batch* b, int32_t steps_per_trial, aerosim_ba
   const aerosim_batch_tuning keep = b->tune;
   aerosim_batch_tuning best = keep;
   best.ms_per_step = 1e300;
-  for (int stages = 2; stages <= 6; ++stages)
-    for (int c = 1; c <= 3; ++c) {
-      aerosim_batch_tuning t{stages, c, 1, 0, 0.0};
-      if (batch_apply_tuning(b, t) != AEROSIM_OK) continue;  // does not fit: skip
-      int rc = aerosim_batch_step(b, 2);
-      if (!rc) rc = aerosim_batch_step(b, steps_per_trial);
-      if (rc) return rc;
-      const double per = b->last_ms / steps_per_trial;
-      if (per < best.ms_per_step) {
-        best = t;
-        best.ms_per_step = per;
+  for (int cells : {256, 512, 1024})
+    for (int stages = 2; stages <= 6; ++stages)
+      for (int c = 1; c <= 3; ++c) {
+        aerosim_batch_tuning t{stages, c, 1, cells, 0.0};
+        if (batch_apply_tuning(b, t) != AEROSIM_OK) continue;  // does not fit: skip
+        int rc = aerosim_batch_step(b, 2);
+        if (!rc) rc = aerosim_batch_step(b, steps_per_trial);
+        if (rc) return rc;
+        const double per = b->last_ms / steps_per_trial;
+        if (per < best.ms_per_step) {
+          best = t;
+          best.ms_per_step = per;
+        }
       }
-    }
   best.graph_steps = keep.graph_steps;
   int rc = batch_apply_tuning(b, best);
   if (rc) return rc;

@@ -402,8 +402,10 @@ class LBMBatch:
         N.check(self.lib.aerosim_batch_autotune(self.h, int(steps_per_trial), C.byref(t)))
         return self._tuning_dict(t)
 
-    def set_tuning(self, stages: int, ctas_per_sm: int, graph_steps: int = 20) -> None:
-        t = N.BatchTuning(int(stages), int(ctas_per_sm), int(graph_steps), 0, 0.0)
+    def set_tuning(self, stages: int, ctas_per_sm: int, graph_steps: int = 20, item_cells: int = 0) -> None:
+        """Launch configuration by hand; item_cells sets the cells per work item (x-rows
+        per item = item_cells / row span, 1..8; 0: 256 cells)."""
+        t = N.BatchTuning(int(stages), int(ctas_per_sm), int(graph_steps), int(item_cells), 0.0)
         N.check(self.lib.aerosim_batch_set_tuning(self.h, C.byref(t)))
 
     def tuning(self) -> dict:
@@ -414,7 +416,7 @@ class LBMBatch:
     @staticmethod
     def _tuning_dict(t) -> dict:
         return {"stages": t.stages, "ctasPerSm": t.ctas_per_sm, "graphSteps": t.graph_steps,
-                "msPerStep": t.ms_per_step}
+                "itemCells": t.item_cells, "msPerStep": t.ms_per_step}
 
     def last_step_timing(self) -> tuple[float, int]:
         ms = C.c_double()

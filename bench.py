@@ -55,8 +55,10 @@ def _peaks():
 
 
 def _profile_traffic(precision: str):
-    """DRAM bytes per step-kernel launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "main_kernel_ellipsoid_256x128x128.md")
+    """DRAM bytes per step-kernel launch from the committed ncu summary, if any (16-bit
+    storage steps run the batched kernel as a batch of one)."""
+    name = "main_kernel_ellipsoid_256x128x128.md" if precision == "f32" else "batch_kernel_ellipsoid_256x128x128_f16s.md"
+    path = os.path.join(ROOT, "profiles", name)
     try:
         text = open(path).read()
     except OSError:

@@ -273,7 +273,8 @@ typedef struct {
   int32_t stages;        /* shared-memory ring slots per CTA (2..6) */
   int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid (1..3) */
   int32_t graph_steps;   /* launches per captured CUDA graph (1: no graph) */
-  int32_t reserved;
+  int32_t item_cells;    /* cells per work item: x-rows per item = clamp(item_cells / row span,
+                            1, 8); 0 = 256 */
   double ms_per_step;    /* autotune: measured time of one batched step */
 } aerosim_batch_tuning;
 
@@ -285,8 +286,9 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
 int aerosim_batch_destroy(aerosim_batch* b);
 /* n steps of every instance; each engine's step count and readouts advance with it. */
 int aerosim_batch_step(aerosim_batch* b, int32_t n);
-/* Times every launch configuration that fits (ring depth x resident CTAs per SM) over
- * steps_per_trial steps each, keeps the fastest, then resets every instance's flow. */
+/* Times every launch configuration that fits (work-item size 256 / 512 / 1024 cells x
+ * ring depth x resident CTAs per SM) over steps_per_trial steps each, keeps the fastest,
+ * then resets every instance's flow. */
 int aerosim_batch_autotune(aerosim_batch* b, int32_t steps_per_trial, aerosim_batch_tuning* out);
 int aerosim_batch_set_tuning(aerosim_batch* b, const aerosim_batch_tuning* t);
 int aerosim_batch_get_tuning(aerosim_batch* b, aerosim_batch_tuning* out);

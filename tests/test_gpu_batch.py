@@ -69,6 +69,32 @@ def test_batch_matches_engines_stepped_alone(oracle_mod, dims):
         ea.close()
 
 
+@pytest.mark.parametrize("item_cells", [512, 1024])
+def test_batch_with_larger_work_items_matches_engines_alone(oracle_mod, item_cells):
+    """Work items of several x-rows (up to 8; the last item of an instance ragged when its
+    row count is not a multiple) step every instance exactly as alone."""
+    dims = [(64, 24, 24), (160, 23, 31), (100, 16, 17)]
+    cs = [_case(nx, ny, nz, 3.0 + k, nx / 3) for k, (nx, ny, nz) in enumerate(dims)]
+    pairs = [(_engine(oracle_mod, c, "f32"), _engine(oracle_mod, c, "f32")) for c in cs]
+    batch = LBMBatch([p[0][1] for p in pairs])
+    t = batch.tuning()
+    batch.set_tuning(2, 1, 5, item_cells)
+    assert batch.tuning()["itemCells"] == item_cells
+    batch.step(40)
+    for (vox, eb), (_, ea) in pairs:
+        ea.step(40)
+        _compare(eb, ea, vox, 1e-5)
+    batch.set_tuning(t["stages"], t["ctasPerSm"], t["graphSteps"], 0)  # back to one-row items mid-run
+    batch.step(10)
+    for (vox, eb), (_, ea) in pairs:
+        ea.step(10)
+        _compare(eb, ea, vox, 1e-5)
+    batch.close()
+    for (_, eb), (_, ea) in pairs:
+        eb.close()
+        ea.close()
+
+
 def test_batch_graph_replay_equals_single_launches(oracle_mod):
     """graph_steps = 5 over 12 steps (two replays and two single launches) against
     graph_steps = 1 (every step its own launch), FP16 storage."""
@@ -98,6 +124,7 @@ def test_batch_autotune_picks_a_fitting_configuration_and_resets(oracle_mod):
     batch.step(5)
     t = batch.autotune(4)
     assert 2 <= t["stages"] <= 6 and 1 <= t["ctasPerSm"] <= 3 and t["msPerStep"] > 0
+    assert t["itemCells"] in (256, 512, 1024)
     for _, e in es:
         assert e.get_step_count() == 0
     batch.step(10)
