@@ -57,7 +57,6 @@ struct aerosim_engine {
   void* staging = nullptr;
   size_t staging_bytes = 0;
   double* frame_host = nullptr;  // pinned: force sums [8] and the device error flag of a frame
-  aerosim_batch* solo = nullptr;  // 16-bit storage: this lattice as a batch of one (see solo_enqueue)
   long long step_index = 0;
   double last_ms = 0;
   long long last_launches = 0;
@@ -68,10 +67,6 @@ struct aerosim_engine {
 };
 
 namespace {
-
-void solo_release(aerosim_engine* h);
-int solo_enqueue(aerosim_engine* h, int32_t n, long long* launches);
-bool solo_eligible(const aerosim_engine* h);
 
 std::string g_create_error;
 std::mutex g_error_mu;
@@ -101,7 +96,6 @@ void free_grid(DevGrid& g) {
 }
 
 void free_pops(aerosim_engine* h) {
-  solo_release(h);
   cudaFree(h->f[0]); cudaFree(h->f[1]);
   h->f[0] = h->f[1] = nullptr;
   cudaFree(h->mux); cudaFree(h->muy); cudaFree(h->muz); cudaFree(h->mrho);
@@ -144,12 +138,13 @@ int configure_step(aerosim_engine* h) {
   dummy.L = L;  // the kernel instance depends on the row pitch and the closure
   dummy.mlp_frag = h->mlp_frag;
   const bool mlp = h->mlp_frag != nullptr;
+  const int groups = step_item_groups_of(h->cfg.precision, mlp);
   const char* env = getenv("AEROSIM_STAGES");
   const int forced = env ? atoi(env) : 0;
   int best_s = 0, best_occ = 0;
   for (int S = 2; S <= 8; ++S) {
     if (forced && S != forced) continue;
-    const size_t smem = step_smem_bytes(L, S, eb, mlp);
+    const size_t smem = step_smem_bytes(L, S, eb, mlp, groups);
     if (smem > 227 * 1024) break;
     int occ = 0;
     cudaError_t e = launch_step(h->cfg.precision, dummy, block, 0, smem, h->stream, &occ, nullptr);
@@ -163,11 +158,12 @@ int configure_step(aerosim_engine* h) {
   if (best_s == 0) return fail(h, AEROSIM_ERR_ARG, "step kernel: no launch configuration fits shared memory");
   h->block = block;
   h->stages = best_s;
-  h->smem = step_smem_bytes(L, best_s, eb, mlp);
+  h->smem = step_smem_bytes(L, best_s, eb, mlp, groups);
   // the occupancy of the chosen configuration
   CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ, nullptr));
   h->occupancy = best_occ;
-  const long long items = ((long long)L.ny * L.nz + rows_per_item(L.nx) - 1) / rows_per_item(L.nx);
+  const long long item_rows = (long long)rows_per_item(L.nx) * groups;
+  const long long items = ((long long)L.ny * L.nz + item_rows - 1) / item_rows;
   long long grid = (long long)best_occ * h->num_sms;
   const char* genv = getenv("AEROSIM_CTAS_PER_SM");
   if (genv && atoi(genv) > 0 && atoi(genv) <= best_occ) grid = (long long)atoi(genv) * h->num_sms;
@@ -231,7 +227,6 @@ int upload_tables(aerosim_engine* h) {
 
 // Installs a freshly built device grid (voxelizer output or host upload).
 int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[3], int reset_flow) {
-  solo_release(h);  // its near-wall list and item table belong to the previous grid
   // A pending rescale belongs to the old flags: apply it before they change.
   if (h->have_grid && h->f[0] && !reset_flow) {
     CU(h, launch_materialize(h->f_prec, h->f[h->cur], h->g.cls, h->st, prev_slot(h), h->L, h->g.N,
@@ -432,7 +427,6 @@ int aerosim_destroy(aerosim_engine* h) {
   if (!h) return AEROSIM_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  solo_release(h);
   free_grid(h->g);
   free_pops(h);
   cudaFree(h->abl); cudaFree(h->sin_tab); cudaFree(h->st);
@@ -634,29 +628,21 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.mlp_nu0 = (float)((std::max(a.tau0, 0.5015) - 0.5) / 3.0);
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
-  if (solo_eligible(h)) {
-    int rc = solo_enqueue(h, n, &launches);
-    if (rc) return rc;
-  } else {
-    for (int s = 0; s < n; ++s) {
-      a.fsrc = h->f[h->cur];
-      a.fdst = h->f[h->cur ^ 1];
-      a.step_index = (int)h->step_index;
-      a.write_macro = (s == n - 1) ? 1 : 0;
-      int nl = 0;
-      CU(h, launch_step(h->cfg.precision, a, h->block, h->grid, h->smem, h->stream, nullptr, &nl));
-      launches += nl;
-      h->cur ^= 1;
-      h->step_index += 1;
-    }
+  for (int s = 0; s < n; ++s) {
+    a.fsrc = h->f[h->cur];
+    a.fdst = h->f[h->cur ^ 1];
+    a.step_index = (int)h->step_index;
+    a.write_macro = (s == n - 1) ? 1 : 0;
+    int nl = 0;
+    CU(h, launch_step(h->cfg.precision, a, h->block, h->grid, h->smem, h->stream, nullptr, &nl));
+    launches += nl;
+    h->cur ^= 1;
+    h->step_index += 1;
   }
   CU(h, cudaEventRecord(h->ev1, h->stream));
   h->last_launches = launches;
   return AEROSIM_OK;
 }
-
-// The device flag a step path raises when its shared-memory pipeline timed out.
-int* step_error_flag(aerosim_engine* h);
 
 // Step timing after the stream has drained.
 int finish_steps(aerosim_engine* h, int dev_err) {
@@ -700,7 +686,7 @@ int aerosim_step(aerosim_engine* h, int32_t n) {
   int rc = enqueue_steps(h, n);
   if (rc) return rc;
   int dev_err = 0;
-  CU(h, cudaMemcpyAsync(&dev_err, step_error_flag(h), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaMemcpyAsync(&dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(h, cudaStreamSynchronize(h->stream));
   return finish_steps(h, dev_err);
 }
@@ -941,7 +927,7 @@ extern "C" int aerosim_step_and_extract_slice(aerosim_engine* h, int32_t n, int3
   for (int i = 0; i < 8; ++i) sums[i] = 0.0;
   int rc = enqueue_steps(h, n);
   if (rc) return rc;
-  CU(h, cudaMemcpyAsync(dev_err, step_error_flag(h), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(h, cudaMemcpyAsync(dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (h->g.B > 0 && (rc = enqueue_forces(h, sums))) return rc;
   if (rgba && (rc = enqueue_slice(h, axis, fraction, mode, rgba, width, height))) return rc;
   CU(h, cudaStreamSynchronize(h->stream));
@@ -1037,8 +1023,6 @@ extern "C" {
 int aerosim_set_sgs_mlp(aerosim_engine* h, const float* params) {
   if (!h) return AEROSIM_ERR_ARG;
   CU(h, cudaSetDevice(h->device));
-  CU(h, cudaStreamSynchronize(h->stream));
-  solo_release(h);  // the closure runs in main_kernel
   if (!params) {
     cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
     h->mlp_frag = nullptr;
@@ -1144,7 +1128,6 @@ struct aerosim_batch {
   cudaGraphExec_t graph = nullptr;
   int graph_len = 0;
   int step = 0;
-  bool own_stream = true;  // false for an engine's batch of one, which runs on the engine's stream
   double last_ms = 0;
   long long last_launches = 0;
 };
@@ -1168,7 +1151,7 @@ void batch_free(aerosim_batch* b) {
   cudaFree(b->d_partials); cudaFree(b->d_ticket); cudaFree(b->d_step); cudaFree(b->d_error);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
-  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
+  if (b->stream) cudaStreamDestroy(b->stream);
 }
 
 // The solver arguments of every instance, from its engine's current configuration.
@@ -1336,99 +1319,6 @@ int batch_enqueue(aerosim_batch* b, int n, long long* launches) {
     BCU(launch_batch(b->precision, a, b->pitch, b->grid, b->smem, b->stream, nullptr));
     *launches += 1;
   }
-  return AEROSIM_OK;
-}
-
-// ---- 16-bit storage: the lattice as a batch of one ----------------------------------
-// Engines with FP16S or BF16S storage and no learned closure step through the batched
-// kernel with work items of 1024 cells (4 x-rows of 256): at 256x128x128 that takes
-// 94.9 us per step against 102.4 us for main_kernel, whose work items are single rows
-// (the per-item pipeline round trips are amortised over four times the cells).  The
-// batch runs on the engine's own stream and reads the engine's state; it is rebuilt
-// when the engine's buffers or grid change, and it never resets the flow.
-
-bool solo_eligible(const aerosim_engine* h) {
-  return (h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S) && !h->mlp_frag;
-}
-
-void solo_release(aerosim_engine* h) {
-  if (!h->solo) return;
-  batch_free(h->solo);
-  delete h->solo;
-  h->solo = nullptr;
-}
-
-int* step_error_flag(aerosim_engine* h) { return h->solo && solo_eligible(h) ? h->solo->d_error : &h->st->error; }
-
-int solo_create(aerosim_engine* h) {
-  aerosim_batch* b = new (std::nothrow) aerosim_batch();
-  if (!b) return fail(h, AEROSIM_ERR_NOMEM, "step: out of host memory");
-  b->device = h->device;
-  b->precision = h->cfg.precision;
-  b->eng.assign(1, h);
-  b->num_sms = h->num_sms;
-  b->stream = h->stream;
-  b->own_stream = false;
-  b->cells = h->g.N;
-  b->n_near = h->n_near;
-  const int p = h->L.pitch;
-  b->pitch = (p == 64 || p == 128 || p == 192 || p == 256) ? p : 0;
-  b->step = -1;  // the device step counter is written before the first launch
-  h->solo = b;
-  void* bufs[2] = {h->f[0], h->f[1]};
-  const long long near_begin[2] = {0, h->n_near};
-  CU(h, cudaEventCreate(&b->ev0));
-  CU(h, cudaEventCreate(&b->ev1));
-  CU(h, cudaMalloc(&b->d_inst, sizeof(StepArgs)));
-  CU(h, cudaMalloc(&b->d_bufs, 2 * sizeof(void*)));
-  CU(h, cudaMalloc(&b->d_item_begin, 2 * sizeof(long long)));
-  CU(h, cudaMalloc(&b->d_near_begin, 2 * sizeof(long long)));
-  CU(h, cudaMalloc(&b->d_geo, sizeof(int4)));
-  CU(h, cudaMalloc(&b->d_partials, (size_t)3 * b->num_sms * sizeof(unsigned long long)));
-  CU(h, cudaMalloc(&b->d_ticket, 2 * sizeof(unsigned int)));
-  CU(h, cudaMalloc(&b->d_step, sizeof(int)));
-  CU(h, cudaMalloc(&b->d_error, sizeof(int)));
-  CU(h, cudaMemcpy(b->d_bufs, bufs, sizeof(bufs), cudaMemcpyHostToDevice));
-  CU(h, cudaMemcpy(b->d_near_begin, near_begin, sizeof(near_begin), cudaMemcpyHostToDevice));
-  CU(h, cudaMemset(b->d_error, 0, sizeof(int)));
-  // the first configuration that fits: 1024-cell items, then smaller ones
-  static const aerosim_batch_tuning kTry[] = {{2, 2, 20, 1024, 0.0}, {3, 2, 20, 1024, 0.0}, {2, 1, 20, 1024, 0.0},
-                                              {2, 2, 20, 512, 0.0},  {3, 3, 20, 0, 0.0},    {2, 1, 20, 0, 0.0}};
-  int rc = AEROSIM_ERR_ARG;
-  for (const aerosim_batch_tuning& t : kTry)
-    if ((rc = batch_apply_tuning(b, t)) == AEROSIM_OK) break;
-  if (rc) return fail(h, rc, std::string("step: no batched launch fits: ") + aerosim_last_error(nullptr));
-  return AEROSIM_OK;
-}
-
-// Enqueues n steps of the batch of one on the engine's stream and advances the
-// engine's step count and buffer parity.
-int solo_enqueue(aerosim_engine* h, int32_t n, long long* launches) {
-  if (!h->solo) {
-    int rc = solo_create(h);
-    if (rc) {
-      solo_release(h);
-      return rc;
-    }
-  }
-  aerosim_batch* b = h->solo;
-  if (b->step != h->step_index) {
-    // first launch, or main_kernel / a reset moved the step count: restart the counter
-    // and the CTA tickets at the engine's step
-    const int s0 = (int)h->step_index;
-    CU(h, cudaMemcpyAsync(b->d_step, &s0, sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    CU(h, cudaMemsetAsync(b->d_ticket, 0, 2 * sizeof(unsigned int), h->stream));
-    b->step = s0;
-  }
-  int rc = batch_upload_table(b);
-  if (!rc) rc = batch_enqueue(b, n, launches);
-  if (rc) return fail(h, rc, aerosim_last_error(nullptr));
-  b->step += n;
-  h->step_index += n;
-  h->cur = (int)(h->step_index & 1);
-  // main_kernel's density accumulators (rho_sum[2], ticket[2]) start from zero whenever
-  // it takes over again
-  CU(h, cudaMemsetAsync(h->st, 0, 2 * sizeof(unsigned long long) + 2 * sizeof(unsigned int), h->stream));
   return AEROSIM_OK;
 }
 

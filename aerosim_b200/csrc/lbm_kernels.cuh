@@ -34,6 +34,18 @@ template <class S, int MODE, bool MLP = false>
 constexpr int step_min_blocks() {
   return MODE != MODE_FAST ? 1 : (MLP ? 2 : (sizeof(typename S::T) == 4 ? 3 : 2));
 }
+// Row groups per work item of the step kernel: a work item holds item_groups x
+// rows_per_item(nx) x-rows and every consumer warp takes its segment of each group, so
+// the slot wait and release and the row setup are paid once per item.  The 16-bit
+// storage kernels use items of 4 groups (4 rows of 256 cells: 102.4 -> 84.1 us per step
+// at 256x128x128); FP32 keeps one group, because its larger ring slots would cost a
+// resident CTA per SM (118.6 -> 127.6 us with 2 groups).
+template <class S, int MODE, bool MLP = false>
+constexpr int step_item_groups() {
+  return MODE == MODE_FAST && !MLP && sizeof(typename S::T) == 2 ? 4 : 1;
+}
+// The same choice from the run-time precision (enum aerosim_precision: 2 = F16S, 3 = BF16S).
+inline int step_item_groups_of(int precision, bool mlp) { return !mlp && (precision == 2 || precision == 3) ? 4 : 1; }
 
 struct NearLink;
 
@@ -455,18 +467,19 @@ __host__ __device__ inline int rows_per_item(int nx) { return (kConsumerWarps * 
 
 // Dynamic shared memory of the step kernel, in order: a guard; the ring of `stages`
 // slots, each holding RY row blocks (19 slot rows of `pitch` elements, pulled from
-// their source rows); the class bytes of the slots' destination rows; a guard; a
-// full and an empty mbarrier per slot; the inlet tables ux_in[ny], uy_in[ny]; the
-// row coordinates [stages][RY]; per consumer warp an outlet scratch row of 20
+// their source rows; groups x RY rows with item row groups); the class bytes of the
+// slots' destination rows; a guard; a full and an empty mbarrier per slot; the inlet
+// tables ux_in[ny], uy_in[ny]; the row coordinates [stages][groups x RY]; per consumer warp an outlet scratch row of 20
 // floats; the per-lane direction table (c_x, c_y, c_z, w; slot) of the row-end cells.
-__host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem) {
-  return (size_t)rows_per_item(L.nx) * (19 * (size_t)L.pitch * elem + (size_t)L.pitch);
+__host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem, int groups = 1) {
+  return (size_t)rows_per_item(L.nx) * groups * (19 * (size_t)L.pitch * elem + (size_t)L.pitch);
 }
 constexpr size_t kSmemGuard = 64;
 // With the learned closure: its weight fragments, biases and per-warp staging blocks.
-__host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem, bool mlp = false) {
-  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem) + kSmemGuard + 16 + 16 * (size_t)stages +
-         2 * (size_t)L.ny * sizeof(double) + (size_t)stages * rows_per_item(L.nx) * sizeof(int2) +
+__host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem, bool mlp = false,
+                                                   int groups = 1) {
+  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem, groups) + kSmemGuard + 16 + 16 * (size_t)stages +
+         2 * (size_t)L.ny * sizeof(double) + (size_t)stages * rows_per_item(L.nx) * groups * sizeof(int2) +
          kConsumerWarps * 20 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int) +
          (mlp ? (kMlpFragWords * 32 + kMlpBias + 3 + kConsumerWarps * 128) * 4 : 0);
 }
@@ -891,18 +904,20 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
   const int shift = row_shift(nx), span = row_span(nx), RY = rows_per_item(nx);
   const int wpr = span / 32;
   const long long rows = (long long)ny * nz;
-  const long long n_items = (rows + RY - 1) / RY;
+  constexpr int G = step_item_groups<S, MODE, MLP>();
+  const int RYG = RY * G;  // rows per work item
+  const long long n_items = (rows + RYG - 1) / RYG;
   const int my_count = blockIdx.x < n_items ? (int)((n_items - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
   T* spop = reinterpret_cast<T*>(smem_raw + kSmemGuard);
-  uint8_t* scls = smem_raw + kSmemGuard + (size_t)S_ * RY * 19 * pitch * sizeof(T);
+  uint8_t* scls = smem_raw + kSmemGuard + (size_t)S_ * RYG * 19 * pitch * sizeof(T);
   uint64_t* full = reinterpret_cast<uint64_t*>(
-      (reinterpret_cast<uintptr_t>(scls + (size_t)S_ * RY * pitch + kSmemGuard) + 7) & ~uintptr_t(7));
+      (reinterpret_cast<uintptr_t>(scls + (size_t)S_ * RYG * pitch + kSmemGuard) + 7) & ~uintptr_t(7));
   uint64_t* empty = full + S_;
   double* s_uxi = reinterpret_cast<double*>(empty + S_);
   double* s_uyi = s_uxi + ny;
-  int2* s_row = reinterpret_cast<int2*>(s_uyi + ny);        // [S_][RY] (iy, iz) of the slot's rows
-  float* s_xo = reinterpret_cast<float*>(s_row + S_ * RY);  // [kConsumerWarps][20]
+  int2* s_row = reinterpret_cast<int2*>(s_uyi + ny);        // [S_][RYG] (iy, iz) of the slot's rows
+  float* s_xo = reinterpret_cast<float*>(s_row + S_ * RYG);  // [kConsumerWarps][20]
   float4* s_dcw = reinterpret_cast<float4*>(
       (reinterpret_cast<uintptr_t>(s_xo + kConsumerWarps * 20) + 15) & ~uintptr_t(15));  // [19]
   int* s_dslot = reinterpret_cast<int*>(s_dcw + 19);                                     // [19]
@@ -976,8 +991,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     int issued = 0;
     int s = 0;
     uint32_t ph = 0;  // parity of the slot's current fill
-    long long r0 = (long long)blockIdx.x * RY;
-    const long long r_step = (long long)gridDim.x * RY;
+    long long r0 = (long long)blockIdx.x * RYG;
+    const long long r_step = (long long)gridDim.x * RYG;
     for (int j = 0; j < my_count; ++j, r0 += r_step) {
       if (j >= S_) {  // the slot's previous fill must have been consumed
         const bool ok = mbar_wait(&empty[s], ph ^ 1u, kWaitLimit);
@@ -986,12 +1001,12 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
           break;
         }
       }
-      const int nr = (int)(rows - r0 < RY ? rows - r0 : RY);
+      const int nr = (int)(rows - r0 < RYG ? rows - r0 : RYG);
       if (lane == 0) {
         // row coordinates for the consumers, published by the arrive below
         for (int yy = 0; yy < nr; ++yy) {
           const int r = (int)(r0 + yy);
-          s_row[s * RY + yy] = make_int2(r % ny, r / ny);
+          s_row[s * RYG + yy] = make_int2(r % ny, r / ny);
         }
         mbar_arrive_expect_tx(&full[s], (uint32_t)nr * (19u * slot_bytes + (uint32_t)pitch));
       }
@@ -1001,14 +1016,14 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
         const int yy = c / 10, g = c - yy * 10;
         const long long r = r0 + yy;
         if (g < kGroups) {
-          const int2 yz = s_row[s * RY + yy];
+          const int2 yz = s_row[s * RYG + yy];
           const long long sr =
               clampi(yz.x - group_cy(g), 0, ny - 1) + (long long)ny * clampi(yz.y - group_cz(g), 0, nz - 1);
           const int first = group_first(g);
-          bulk_load(spop + ((size_t)(s * RY + yy) * 19 + first) * pitch, fs + (sr * 19 + first) * pitch,
+          bulk_load(spop + ((size_t)(s * RYG + yy) * 19 + first) * pitch, fs + (sr * 19 + first) * pitch,
                     (uint32_t)group_count(g) * slot_bytes, &full[s]);
         } else {
-          bulk_load(scls + (size_t)(s * RY + yy) * pitch, a.cls + r * pitch, (uint32_t)pitch, &full[s]);
+          bulk_load(scls + (size_t)(s * RYG + yy) * pitch, a.cls + r * pitch, (uint32_t)pitch, &full[s]);
         }
       }
       issued = j + 1;
@@ -1035,10 +1050,10 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     int s = 0;
     uint32_t ph = 0;
     int seg = warp % wpr;  // the row-end segments rotate over the warps of a row
-    long long row = (long long)blockIdx.x * RY + ry;
-    const long long row_step = (long long)gridDim.x * RY;
+    long long row0 = (long long)blockIdx.x * RYG + ry;  // this warp's row of the item's first group
+    const long long row_step = (long long)gridDim.x * RYG;
 
-    for (int j = 0; j < my_count; ++j, row += row_step) {
+    for (int j = 0; j < my_count; ++j, row0 += row_step) {
       {
         const bool ok = mbar_wait(&full[s], ph, kWaitLimit);
         if (!__any_sync(0xffffffffu, ok)) {
@@ -1046,63 +1061,66 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
           break;
         }
       }
-      const bool row_ok = row < rows;
-      int iy = 0, iz = 0;
-      if (row_ok) {
-        const int2 yz = s_row[s * RY + ry];
-        iy = yz.x;
-        iz = yz.y;
-      }
-      const T* sp = spop + (size_t)(s * RY + ry) * 19 * pitch;
-      const uint8_t* sc = scls + (size_t)(s * RY + ry) * pitch;
-      const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
+      for (int gq = 0; gq < G; ++gq) {  // the item's row groups
+        const long long row = row0 + (long long)gq * RY;
+        const bool row_ok = row < rows;
+        int iy = 0, iz = 0;
+        if (row_ok) {
+          const int2 yz = s_row[s * RYG + gq * RY + ry];
+          iy = yz.x;
+          iz = yz.y;
+        }
+        const T* sp = spop + (size_t)(s * RYG + gq * RY + ry) * 19 * pitch;
+        const uint8_t* sc = scls + (size_t)(s * RYG + gq * RY + ry) * pitch;
+        const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
 
-      for (int c = 0; c < nchunks; ++c) {
-        const int cell_lo = c * span + seg * 32 - shift;  // cell of lane 0
-        const int ix = cell_lo + lane;
-        const bool active = row_ok && ix >= 0 && ix < nx;
-        const int lx = (ix >= 0 && ix < nx) ? ix : 1;  // lanes outside the row read cell 1
-        const uint8_t cl = sc[lx];
-        const int flag = cl & CLS_FLAG_MASK;
-        const bool near = (cl & CLS_NEAR) != 0;
-        Real v[19];
-        // ---- pull-stream (lbmCpuReference.ts:189-231) from the staged rows ----
+        for (int c = 0; c < nchunks; ++c) {
+          const int cell_lo = c * span + seg * 32 - shift;  // cell of lane 0
+          const int ix = cell_lo + lane;
+          const bool active = row_ok && ix >= 0 && ix < nx;
+          const int lx = (ix >= 0 && ix < nx) ? ix : 1;  // lanes outside the row read cell 1
+          const uint8_t cl = sc[lx];
+          const int flag = cl & CLS_FLAG_MASK;
+          const bool near = (cl & CLS_NEAR) != 0;
+          Real v[19];
+          // ---- pull-stream (lbmCpuReference.ts:189-231) from the staged rows ----
 #pragma unroll
-        for (int d = 0; d < 19; ++d) {
-          const T raw = sp[slot_of(d) * pitch + lx - cx_of(d)];
-          if constexpr (MODE == MODE_FAST) v[d] = S::h_scaled(raw, d, corrf, corrf_s);
-          else if constexpr (MODE == MODE_MIRROR) v[d] = (double)(float)(S::f_of(raw, d) * corr);
-          else v[d] = S::f_of(raw, d) * corr;
-        }
-        if (c == nchunks - 1) {  // every value of this slot is in registers: release it
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&empty[s]);
-        }
-
-        if constexpr (MODE == MODE_FAST) {
-          SegGeom g;
-          g.row = row; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
-          g.iy = iy; g.iz = iz; g.cell_lo = cell_lo; g.ix = ix; g.flag = flag;
-          g.row_ok = row_ok; g.active = active; g.near = near; g.wall_row = wall_row;
-          g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro; g.cl = cl;
-          auto inlet = [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); };
-          if constexpr (MLP) {
-            const MlpRefs mr{s_mfrag, s_mbias, s_mstage + warp * 128, a.mlp_nu0, 0.0f, lane};
-            fast_segment<S, decltype(inlet), true>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a,
-                                                   s_xo + warp * 20, s_dcw, s_dslot, lane, my_sum, my_nan, &mr);
-          } else {
-            fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a, s_xo + warp * 20, s_dcw, s_dslot,
-                            lane, my_sum, my_nan);
+          for (int d = 0; d < 19; ++d) {
+            const T raw = sp[slot_of(d) * pitch + lx - cx_of(d)];
+            if constexpr (MODE == MODE_FAST) v[d] = S::h_scaled(raw, d, corrf, corrf_s);
+            else if constexpr (MODE == MODE_MIRROR) v[d] = (double)(float)(S::f_of(raw, d) * corr);
+            else v[d] = S::f_of(raw, d) * corr;
           }
-        } else {
-          CellCtx cc;
-          cc.row = row; cc.ix = ix; cc.iy = iy; cc.iz = iz; cc.cell_lo = cell_lo; cc.flag = flag;
-          cc.active = active; cc.near = near;
-          my_sum += general_cells<S, MODE, P>(a, v, cc, s_uxi, s_uyi, &my_nan);
+          if (gq == G - 1 && c == nchunks - 1) {  // every value of this slot is in registers: release it
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+          }
+
+          if constexpr (MODE == MODE_FAST) {
+            SegGeom g;
+            g.row = row; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
+            g.iy = iy; g.iz = iz; g.cell_lo = cell_lo; g.ix = ix; g.flag = flag;
+            g.row_ok = row_ok; g.active = active; g.near = near; g.wall_row = wall_row;
+            g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro; g.cl = cl;
+            auto inlet = [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); };
+            if constexpr (MLP) {
+              const MlpRefs mr{s_mfrag, s_mbias, s_mstage + warp * 128, a.mlp_nu0, 0.0f, lane};
+              fast_segment<S, decltype(inlet), true>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a,
+                                                     s_xo + warp * 20, s_dcw, s_dslot, lane, my_sum, my_nan, &mr);
+            } else {
+              fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a, s_xo + warp * 20, s_dcw, s_dslot,
+                              lane, my_sum, my_nan);
+            }
+          } else {
+            CellCtx cc;
+            cc.row = row; cc.ix = ix; cc.iy = iy; cc.iz = iz; cc.cell_lo = cell_lo; cc.flag = flag;
+            cc.active = active; cc.near = near;
+            my_sum += general_cells<S, MODE, P>(a, v, cc, s_uxi, s_uyi, &my_nan);
+          }
         }
+        if (++seg == wpr) seg = 0;
       }
       if (++s == S_) { s = 0; ph ^= 1u; }
-      if (++seg == wpr) seg = 0;
     }
     if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
     if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);

@@ -55,9 +55,10 @@ def _peaks():
 
 
 def _profile_traffic(precision: str):
-    """DRAM bytes per step-kernel launch from the committed ncu summary, if any (16-bit
-    storage steps run the batched kernel as a batch of one)."""
-    name = "main_kernel_ellipsoid_256x128x128.md" if precision == "f32" else "batch_kernel_ellipsoid_256x128x128_f16s.md"
+    """DRAM bytes per step-kernel launch from the committed ncu summary, if any (the 16-bit
+    storage kernels run with 4-row work items)."""
+    name = ("main_kernel_ellipsoid_256x128x128.md" if precision == "f32"
+            else "main_kernel_f16s_4row_items_ellipsoid_256x128x128.md")
     path = os.path.join(ROOT, "profiles", name)
     try:
         text = open(path).read()
