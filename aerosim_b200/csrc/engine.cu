@@ -39,6 +39,7 @@ struct aerosim_engine {
   unsigned grid = 1;
   size_t smem = 0;
   int stages = 3;
+  int item_groups = 1;  // row groups per work item of the step kernel
   int occupancy = 0;
   int num_sms = 148;
   float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
@@ -138,7 +139,8 @@ int configure_step(aerosim_engine* h) {
   dummy.L = L;  // the kernel instance depends on the row pitch and the closure
   dummy.mlp_frag = h->mlp_frag;
   const bool mlp = h->mlp_frag != nullptr;
-  const int groups = step_item_groups_of(h->cfg.precision, mlp);
+  const bool grouped = !mlp && (h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S);
+  const int groups = grouped ? item_groups_for(L.nx) : 1;
   const char* env = getenv("AEROSIM_STAGES");
   const int forced = env ? atoi(env) : 0;
   int best_s = 0, best_occ = 0;
@@ -159,6 +161,7 @@ int configure_step(aerosim_engine* h) {
   h->block = block;
   h->stages = best_s;
   h->smem = step_smem_bytes(L, best_s, eb, mlp, groups);
+  h->item_groups = groups;
   // the occupancy of the chosen configuration
   CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ, nullptr));
   h->occupancy = best_occ;
@@ -626,6 +629,7 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.mlp_frag = h->mlp_frag;
   a.mlp_bias = h->mlp_bias;
   a.mlp_nu0 = (float)((std::max(a.tau0, 0.5015) - 0.5) / 3.0);
+  a.item_groups = h->item_groups;
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < n; ++s) {

@@ -37,15 +37,14 @@ constexpr int step_min_blocks() {
 // Row groups per work item of the step kernel: a work item holds item_groups x
 // rows_per_item(nx) x-rows and every consumer warp takes its segment of each group, so
 // the slot wait and release and the row setup are paid once per item.  The 16-bit
-// storage kernels use items of 4 groups (4 rows of 256 cells: 102.4 -> 84.1 us per step
-// at 256x128x128); FP32 keeps one group, because its larger ring slots would cost a
-// resident CTA per SM (118.6 -> 127.6 us with 2 groups).
+// storage kernels take items of about 1024 cells (4 rows of 256 cells: 102.4 -> 85.1 us
+// per step at 256x128x128; the group count is StepArgs::item_groups); FP32 keeps one
+// group, because its larger ring slots would cost a resident CTA per SM (118.6 -> 127.6
+// us with 2 groups).
 template <class S, int MODE, bool MLP = false>
-constexpr int step_item_groups() {
-  return MODE == MODE_FAST && !MLP && sizeof(typename S::T) == 2 ? 4 : 1;
+constexpr bool step_item_grouped() {
+  return MODE == MODE_FAST && !MLP && sizeof(typename S::T) == 2;
 }
-// The same choice from the run-time precision (enum aerosim_precision: 2 = F16S, 3 = BF16S).
-inline int step_item_groups_of(int precision, bool mlp) { return !mlp && (precision == 2 || precision == 3) ? 4 : 1; }
 
 struct NearLink;
 
@@ -77,6 +76,7 @@ struct StepArgs {
   const uint32_t* mlp_frag;
   const float* mlp_bias;
   float mlp_nu0;
+  int item_groups;        // row groups per work item (16-bit storage kernels; 1 elsewhere)
 };
 
 struct ForceArgs {
@@ -464,6 +464,12 @@ __host__ __device__ inline int row_span(int nx) {  // threads along x (multiple 
   return t > kConsumerWarps * 32 ? kConsumerWarps * 32 : t;
 }
 __host__ __device__ inline int rows_per_item(int nx) { return (kConsumerWarps * 32) / row_span(nx); }
+// Row groups per work item for about 1024 cells per item (1..4).
+__host__ __device__ inline int item_groups_for(int nx) {
+  const int span = row_span(nx), chunks = (nx + row_shift(nx) + span - 1) / span;
+  const int cells = rows_per_item(nx) * chunks * span;
+  return cells >= 1024 ? 1 : (1024 / cells > 4 ? 4 : 1024 / cells);
+}
 
 // Dynamic shared memory of the step kernel, in order: a guard; the ring of `stages`
 // slots, each holding RY row blocks (19 slot rows of `pitch` elements, pulled from
@@ -904,7 +910,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
   const int shift = row_shift(nx), span = row_span(nx), RY = rows_per_item(nx);
   const int wpr = span / 32;
   const long long rows = (long long)ny * nz;
-  constexpr int G = step_item_groups<S, MODE, MLP>();
+  const int G = step_item_grouped<S, MODE, MLP>() && a.item_groups > 1 ? a.item_groups : 1;
   const int RYG = RY * G;  // rows per work item
   const long long n_items = (rows + RYG - 1) / RYG;
   const int my_count = blockIdx.x < n_items ? (int)((n_items - 1 - blockIdx.x) / gridDim.x + 1) : 0;

@@ -95,6 +95,24 @@ def test_batch_with_larger_work_items_matches_engines_alone(oracle_mod, item_cel
         ea.close()
 
 
+def test_fp16_engines_alone_match_a_batch_across_widths(oracle_mod):
+    """The 16-bit step kernel's multi-row work items (about 1024 cells: 4 to 32 rows, the
+    last item of a lattice ragged) against the batched kernel's own item walk: each
+    engine stepped alone equals its instance in a batch."""
+    dims = [(33, 12, 10), (65, 10, 9), (100, 12, 7), (160, 9, 10), (300, 8, 9)]
+    cs = [_case(nx, ny, nz, 2.5, nx / 3) for nx, ny, nz in dims]
+    pairs = [(_engine(oracle_mod, c, "f16s"), _engine(oracle_mod, c, "f16s")) for c in cs]
+    batch = LBMBatch([p[0][1] for p in pairs])
+    batch.step(50)
+    for (vox, eb), (_, ea) in pairs:
+        ea.step(50)
+        _compare(eb, ea, vox, 1e-5, atol=1e-6)
+    batch.close()
+    for (_, eb), (_, ea) in pairs:
+        eb.close()
+        ea.close()
+
+
 def test_batch_graph_replay_equals_single_launches(oracle_mod):
     """graph_steps = 5 over 12 steps (two replays and two single launches) against
     graph_steps = 1 (every step its own launch), FP16 storage."""
