@@ -61,15 +61,25 @@ class ForceConvergenceTracker:
     def __init__(self) -> None:
         self.window_size = 60
         self.samples: list[_Sample] = []
+        self._history: list[dict] = []  # readout history entries, kept in step with samples
+        self._history_q = None          # the q_inf * A_ref they were computed with
 
     def reset(self, window_size: int = 60) -> None:
         self.window_size = window_size
         self.samples = []
+        self._history = []
+        self._history_q = None
+
+    @staticmethod
+    def _entry(s: _Sample, q_area: float) -> dict:
+        return {"step": s.step, "cd": s.cd, "cl": s.cl, "cm": s.cm, "xcp": s.xcp,
+                "dragForceN": s.cd * q_area, "liftForceN": s.cl * q_area}
 
     def push_sample(self, step: int, cd: float, cl: float, cm: float, xcp: float, wind_speed: float,
                     fluid: dict, frontal_area_m2: float) -> dict:
         self.samples.append(_Sample(step, cd, cl, cm, xcp))
-        if len(self.samples) > 180:
+        dropped = len(self.samples) > 180
+        if dropped:
             self.samples.pop(0)
         recent = self.samples[-self.window_size:]
         n = len(recent)
@@ -94,8 +104,20 @@ class ForceConvergenceTracker:
             "dragForceKgf": drag_n * NEWTONS_TO_KGF, "liftForceNewtons": lift_n,
             "liftForceLbs": lift_n * NEWTONS_TO_LBF, "pitchingMomentCm": mean_cm,
             "centerOfPressureX": mean_xcp, "stabilityPercent": stability, "isConverged": converged,
-            "history": [{"step": s.step, "cd": s.cd, "cl": s.cl, "cm": s.cm, "xcp": s.xcp,
-                         "dragForceN": s.cd * q_area, "liftForceN": s.cl * q_area} for s in self.samples],
+            "history": self._history_list(q_area, dropped),
         }
+
+    def _history_list(self, q_area: float, dropped: bool) -> list:
+        """The per-sample entries of every readout (forces from this call's q_inf * A_ref),
+        updated by one entry per sample instead of rebuilt; the entries are shared between
+        readouts and must be treated as read-only."""
+        if q_area != self._history_q or len(self._history) != len(self.samples) - 1 + dropped:
+            self._history = [self._entry(s, q_area) for s in self.samples]
+            self._history_q = q_area
+        else:
+            if dropped:
+                self._history.pop(0)
+            self._history.append(self._entry(self.samples[-1], q_area))
+        return list(self._history)
 
     pushSample = push_sample

@@ -191,3 +191,19 @@ def test_history_from_readout():
     assert hist[4]["xcpMeters"] == 0.3 and hist[0]["cm"] == 0.02
     csv = telemetry.export_telemetry_to_csv(hist, {"specimenName": "s"})
     assert csv.split("\r\n")[-1].startswith("500,0.5000,0.54000,0.10000,0.02000,")
+
+
+def test_tracker_history_matches_a_full_rebuild():
+    """The readout history is kept entry by entry (180 samples at most); it equals the
+    list built from all samples with the call's q_inf * A_ref, also after q changes."""
+    tr = forces.ForceConvergenceTracker()
+    rng = random.Random(5)
+    for i in range(400):
+        u = 20.0 if i < 300 else 25.0
+        r = tr.push_sample(4 * i, rng.random(), rng.random() - 0.5, 0.01, 0.3, u, forces.AIR_20C, 0.25)
+        q = 0.5 * forces.AIR_20C["density"] * u * u * 0.25
+        if i % 37 == 0 or i in (179, 180, 181, 300, 399):
+            ref = [{"step": s.step, "cd": s.cd, "cl": s.cl, "cm": s.cm, "xcp": s.xcp,
+                    "dragForceN": s.cd * q, "liftForceN": s.cl * q} for s in tr.samples]
+            assert r["history"] == ref
+    assert len(r["history"]) == 180 and r["history"][0]["step"] == 4 * 220
