@@ -110,13 +110,20 @@ __device__ __forceinline__ uint32_t bf16x2_of(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t*>(&v);
 }
-__device__ __forceinline__ float tanh_approx(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float gelu_fast(float x) {
-  return 0.5f * x * (1.0f + tanh_approx(kGeluK * fmaf(0.044715f * x, x * x, x)));
+// GELU of two pre-activations as one packed BF16 pair, the operand type of the next
+// layer: the pair is rounded to BF16 first and the tanh form is evaluated in bf16x2
+// arithmetic (x/2 (1 + tanh(x (k + k c x^2))), k = sqrt(2/pi) and k c = k * 0.044715 as
+// BF16 constants 0x3f4c and 0x3d12), about a third of the instructions of two FP32 GELUs.
+__device__ __forceinline__ uint32_t gelu_bf16x2(float a, float b) {
+  const uint32_t x = bf16x2_of(a, b);
+  uint32_t x2, u, t, r;
+  asm("mul.rn.bf16x2 %0, %1, %1;" : "=r"(x2) : "r"(x));
+  asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(u) : "r"(x2), "r"(0x3d123d12u), "r"(0x3f4c3f4cu));
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(u) : "r"(u), "r"(x));
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(u));
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(u) : "r"(x), "r"(0x3f003f00u));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(r) : "r"(u), "r"(t));
+  return r;
 }
 
 // nu_t / nu_0 of this lane's cell.  All 32 lanes must call it together.  x: the lane's
@@ -156,10 +163,10 @@ __device__ __forceinline__ float mlp_nut_warp(const float (&x)[kMlpIn], const ui
     for (int kt = 0; kt < 2; ++kt) {
       const float* lo = h[mt][2 * kt];
       const float* hi = h[mt][2 * kt + 1];
-      a2[mt][kt][0] = bf16x2_of(gelu_fast(lo[0]), gelu_fast(lo[1]));
-      a2[mt][kt][1] = bf16x2_of(gelu_fast(lo[2]), gelu_fast(lo[3]));
-      a2[mt][kt][2] = bf16x2_of(gelu_fast(hi[0]), gelu_fast(hi[1]));
-      a2[mt][kt][3] = bf16x2_of(gelu_fast(hi[2]), gelu_fast(hi[3]));
+      a2[mt][kt][0] = gelu_bf16x2(lo[0], lo[1]);
+      a2[mt][kt][1] = gelu_bf16x2(lo[2], lo[3]);
+      a2[mt][kt][2] = gelu_bf16x2(hi[0], hi[1]);
+      a2[mt][kt][3] = gelu_bf16x2(hi[2], hi[3]);
     }
   // layer 2: 32 -> 32
 #pragma unroll
@@ -184,10 +191,10 @@ __device__ __forceinline__ float mlp_nut_warp(const float (&x)[kMlpIn], const ui
     for (int kt = 0; kt < 2; ++kt) {
       const float* lo = h[mt][2 * kt];
       const float* hi = h[mt][2 * kt + 1];
-      a2[mt][kt][0] = bf16x2_of(gelu_fast(lo[0]), gelu_fast(lo[1]));
-      a2[mt][kt][1] = bf16x2_of(gelu_fast(lo[2]), gelu_fast(lo[3]));
-      a2[mt][kt][2] = bf16x2_of(gelu_fast(hi[0]), gelu_fast(hi[1]));
-      a2[mt][kt][3] = bf16x2_of(gelu_fast(hi[2]), gelu_fast(hi[3]));
+      a2[mt][kt][0] = gelu_bf16x2(lo[0], lo[1]);
+      a2[mt][kt][1] = gelu_bf16x2(lo[2], lo[3]);
+      a2[mt][kt][2] = gelu_bf16x2(hi[0], hi[1]);
+      a2[mt][kt][3] = gelu_bf16x2(hi[2], hi[3]);
     }
   // layer 3: 32 -> 1 (N padded to 8; column 0 is the output)
   float o[2][4];

@@ -118,15 +118,15 @@ __device__ __forceinline__ bool umma_mbar_wait(uint32_t mbar_smem, uint32_t pari
   return false;
 }
 
-// GELU(d + b) of 32 columns, stored as BF16 into row r of a K = 32 operand.
+// GELU(d + b) of 32 columns (packed BF16 pairs), stored into row r of a K = 32 operand.
 __device__ __forceinline__ void umma_store_hidden(uint8_t* A, int r, const float (&d)[32], const float* b) {
 #pragma unroll
   for (int g = 0; g < 4; ++g) {
     uint4 w;
-    w.x = bf16x2_of(gelu_fast(d[8 * g + 0] + b[8 * g + 0]), gelu_fast(d[8 * g + 1] + b[8 * g + 1]));
-    w.y = bf16x2_of(gelu_fast(d[8 * g + 2] + b[8 * g + 2]), gelu_fast(d[8 * g + 3] + b[8 * g + 3]));
-    w.z = bf16x2_of(gelu_fast(d[8 * g + 4] + b[8 * g + 4]), gelu_fast(d[8 * g + 5] + b[8 * g + 5]));
-    w.w = bf16x2_of(gelu_fast(d[8 * g + 6] + b[8 * g + 6]), gelu_fast(d[8 * g + 7] + b[8 * g + 7]));
+    w.x = gelu_bf16x2(d[8 * g + 0] + b[8 * g + 0], d[8 * g + 1] + b[8 * g + 1]);
+    w.y = gelu_bf16x2(d[8 * g + 2] + b[8 * g + 2], d[8 * g + 3] + b[8 * g + 3]);
+    w.z = gelu_bf16x2(d[8 * g + 4] + b[8 * g + 4], d[8 * g + 5] + b[8 * g + 5]);
+    w.w = gelu_bf16x2(d[8 * g + 6] + b[8 * g + 6], d[8 * g + 7] + b[8 * g + 7]);
     *reinterpret_cast<uint4*>(A + umma_off(r, 8 * g, 32)) = w;
   }
 }
