@@ -143,6 +143,10 @@ def test_batch_autotune_picks_a_fitting_configuration_and_resets(oracle_mod):
     t = batch.autotune(4)
     assert 2 <= t["stages"] <= 6 and 1 <= t["ctasPerSm"] <= 3 and t["msPerStep"] > 0
     assert t["itemCells"] in (256, 512, 1024)
+    with pytest.raises(AerosimError) as err:  # work items above 2048 cells are refused
+        batch.set_tuning(2, 1, 5, 4096)
+    assert err.value.code == N.ERR_ARG
+    assert batch.tuning()["itemCells"] == t["itemCells"]
     for _, e in es:
         assert e.get_step_count() == 0
     batch.step(10)
