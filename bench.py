@@ -251,6 +251,8 @@ def run_ours(args) -> dict:
     # ---- batched sweep: 32 wings of uneven lattice sizes, one launch per step ----
     if args.batch_steps > 0:
         out["batch"] = run_batch(args, dev, ws, barrier_sync, max_over_ranks)
+        if ws > 1:  # the same 32-wing sweep split round-robin over the ranks (no exchange)
+            out["batch_sharded"] = run_batch(args, dev, ws, barrier_sync, max_over_ranks, shard=(rank, ws))
 
     # ---- Cd / Cl / Cm error of reduced storage vs the FP64 GPU run.  The flow at
     # Re = 2e4 is unsteady and chaotic: runs that differ only in rounding follow each
@@ -355,14 +357,18 @@ def closure_forward_tiles(params, rows: int, reps: int = 3) -> dict:
     return res
 
 
-def run_batch(args, dev: int, ws: int, barrier_sync, max_over_ranks) -> dict:
+def run_batch(args, dev: int, ws: int, barrier_sync, max_over_ranks, shard=None) -> dict:
     """The batched angle-of-attack sweep (32 extruded NACA 0012 wings, lattices
     128x64x64 .. 190x95x95, FP16 shifted storage) in one persistent launch per step:
     autotuned launch configuration, device-timed steps, per-instance Cd / Cl averaged
-    over the last fifth of the run (a force sample every 200 steps)."""
+    over the last fifth of the run (a force sample every 200 steps).  Every rank runs the
+    whole sweep (weak scaling), or with shard = (rank, world) its round-robin share of
+    the wings, and `mlups` is then the whole sweep's cells over the slowest rank's time."""
     from aerosim_b200 import LBMBatch
-    from aerosim_b200 import cases
+    from aerosim_b200 import cases, distributed
     cs = cases.naca_batch(steps=args.batch_steps)
+    if shard is not None:
+        cs = distributed.shard(cs, shard[0], shard[1])
     engines, vox_ms = [], 0.0
     for c in cs:
         e, info = _make_engine(c, "f16s", dev)
@@ -396,12 +402,14 @@ def run_batch(args, dev: int, ws: int, barrier_sync, max_over_ranks) -> dict:
     total_ms = max_over_ranks(total_ms)
     nan = any(e.mass_stats()["hasNaN"] for e in engines)
     cells = b.cells
+    sweep_cells = distributed.sum_over_ranks(float(cells), device=f"cuda:{dev}") if shard is not None else ws * cells
     b.close()
     for e in engines:
         e.close()
     return {"workload": f"naca0012_x{len(cs)}_128x64x64..190x95x95_f16s", "instances": len(cs),
             "cells_per_gpu": cells, "steps": args.batch_steps,
-            "mlups": round(ws * cells * args.batch_steps / (total_ms * 1e-3) / 1e6, 1),
+            "scaling": "strong (instances sharded over the ranks)" if shard is not None else "weak",
+            "mlups": round(sweep_cells * args.batch_steps / (total_ms * 1e-3) / 1e6, 1),
             "ms_per_step": total_ms / args.batch_steps, "gpu_launches": int(launches),
             "tuning": tune, "voxelization_ms_total": round(vox_ms, 1),
             "aoa_deg": [round(c.extra["aoa_deg"], 2) for c in cs],
