@@ -914,6 +914,12 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
   const int RYG = RY * G;  // rows per work item
   const long long n_items = (rows + RYG - 1) / RYG;
   const int my_count = blockIdx.x < n_items ? (int)((n_items - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  // Odd steps take the items last to first: a step then begins on the rows the step
+  // before wrote last, while they are still in L2.  Every cell's update reads only the
+  // source lattice and the density sums are fixed-point, so the order changes no result.
+  const bool reverse = (a.step_index & 1) != 0;
+  const long long item_row0 = (reverse ? n_items - 1 - blockIdx.x : (long long)blockIdx.x) * RYG;
+  const long long item_step = reverse ? -(long long)gridDim.x * RYG : (long long)gridDim.x * RYG;
 
   T* spop = reinterpret_cast<T*>(smem_raw + kSmemGuard);
   uint8_t* scls = smem_raw + kSmemGuard + (size_t)S_ * RYG * 19 * pitch * sizeof(T);
@@ -997,9 +1003,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     int issued = 0;
     int s = 0;
     uint32_t ph = 0;  // parity of the slot's current fill
-    long long r0 = (long long)blockIdx.x * RYG;
-    const long long r_step = (long long)gridDim.x * RYG;
-    for (int j = 0; j < my_count; ++j, r0 += r_step) {
+    long long r0 = item_row0;  // first row of this CTA's j-th item
+    for (int j = 0; j < my_count; ++j, r0 += item_step) {
       if (j >= S_) {  // the slot's previous fill must have been consumed
         const bool ok = mbar_wait(&empty[s], ph ^ 1u, kWaitLimit);
         if (!__any_sync(0xffffffffu, ok)) {
@@ -1056,10 +1061,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     int s = 0;
     uint32_t ph = 0;
     int seg = warp % wpr;  // the row-end segments rotate over the warps of a row
-    long long row0 = (long long)blockIdx.x * RYG + ry;  // this warp's row of the item's first group
-    const long long row_step = (long long)gridDim.x * RYG;
-
-    for (int j = 0; j < my_count; ++j, row0 += row_step) {
+    long long row0 = item_row0 + ry;  // this warp's row of the item's first group
+    for (int j = 0; j < my_count; ++j, row0 += item_step) {
       {
         const bool ok = mbar_wait(&full[s], ph, kWaitLimit);
         if (!__any_sync(0xffffffffu, ok)) {
