@@ -83,13 +83,22 @@ class ForceConvergenceTracker:
             self.samples.pop(0)
         recent = self.samples[-self.window_size:]
         n = len(recent)
-        mean_cd = sum(s.cd for s in recent) / n
-        mean_cl = sum(s.cl for s in recent) / n
-        mean_cm = sum(s.cm for s in recent) / n
-        mean_xcp = sum(s.xcp for s in recent) / n
+        # plain left-to-right sums as the reference adds them (:355-366); Python's sum()
+        # of floats compensates the rounding and can differ in the last bit
+        sum_cd = sum_cl = sum_cm = sum_xcp = 0.0
+        for s in recent:
+            sum_cd += s.cd
+            sum_cl += s.cl
+            sum_cm += s.cm
+            sum_xcp += s.xcp
+        mean_cd = sum_cd / n
+        mean_cl = sum_cl / n
+        mean_cm = sum_cm / n
+        mean_xcp = sum_xcp / n
         var_cd = 0.0
         for s in recent:
-            var_cd += (s.cd - mean_cd) ** 2
+            diff = s.cd - mean_cd
+            var_cd += diff * diff
         std_cd = math.sqrt(var_cd / max(1, n))
         rel_std = std_cd / max(0.02, abs(mean_cd))
         fill = min(1.0, n / 25)

@@ -207,3 +207,18 @@ def test_tracker_history_matches_a_full_rebuild():
                     "dragForceN": s.cd * q, "liftForceN": s.cl * q} for s in tr.samples]
             assert r["history"] == ref
     assert len(r["history"]) == 180 and r["history"][0]["step"] == 4 * 220
+
+
+def test_tracker_means_are_plain_left_to_right_sums():
+    """forceIntegrator.ts:355-377 adds the window's samples in order with no compensation:
+    1e16 + 1 rounds back to 1e16, so the window {1e16, 1, -1e16} has mean 0, not 1/3."""
+    tr = forces.ForceConvergenceTracker()
+    for i, cd in enumerate((1e16, 1.0, -1e16)):
+        r = tr.push_sample(i, cd, cd, cd, cd, 20.0, forces.AIR_20C, 0.25)
+    assert r["meanCd"] == 0.0 and r["meanCl"] == 0.0 and r["pitchingMomentCm"] == 0.0
+    assert r["centerOfPressureX"] == 0.0
+    # the variance adds diff * diff in the same order: (1e16)^2 + 1 + (1e16)^2 over 3
+    var = 0.0
+    for cd in (1e16, 1.0, -1e16):
+        var += cd * cd
+    assert r["stdCd"] == math.sqrt(var / 3)
