@@ -63,6 +63,13 @@ struct StoreF32 {
   using T = float;
   // FP32-collision output in the storage domain: value = kOutScale * h + kOutW * w_d
   static constexpr float kOutScale = 1.0f, kOutW = 1.0f;
+  // kRawMoments: the collision takes the stored values as they are (raw()) and applies
+  // the storage scale kRawScale and the pending rescale to its ten moments instead of
+  // to the 19 values (stored deviations only: a full f would lose its small moments
+  // to cancellation against the rest weights)
+  static constexpr bool kRawMoments = false;
+  static constexpr float kRawScale = 1.0f;
+  __device__ __forceinline__ static float raw(T v) { return v; }
   __device__ __forceinline__ static T store(float v) { return v; }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
     return fmaf(v, corr, -wf_of(d));
@@ -75,6 +82,9 @@ struct StoreF32 {
 struct StoreF64 {
   using T = double;
   static constexpr float kOutScale = 1.0f, kOutW = 1.0f;
+  static constexpr bool kRawMoments = false;
+  static constexpr float kRawScale = 1.0f;
+  __device__ __forceinline__ static float raw(T v) { return (float)v; }
   __device__ __forceinline__ static T store(float v) { return (double)v; }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
     return (float)(v * (double)corr - w64_of(d));
@@ -87,6 +97,9 @@ struct StoreF64 {
 struct StoreF16S {
   using T = __half;
   static constexpr float kOutScale = F16S_SCALE, kOutW = 0.0f;
+  static constexpr bool kRawMoments = true;
+  static constexpr float kRawScale = F16S_INV_SCALE;
+  __device__ __forceinline__ static float raw(T v) { return __half2float(v); }
   __device__ __forceinline__ static T store(float v) { return __float2half_rn(v); }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float corr_s) {
     return fmaf(__half2float(v), corr_s, wf_of(d) * (corr - 1.0f));
@@ -99,6 +112,9 @@ struct StoreF16S {
 struct StoreBF16S {
   using T = __nv_bfloat16;
   static constexpr float kOutScale = 1.0f, kOutW = 0.0f;
+  static constexpr bool kRawMoments = true;
+  static constexpr float kRawScale = 1.0f;
+  __device__ __forceinline__ static float raw(T v) { return __bfloat162float(v); }
   __device__ __forceinline__ static T store(float v) { return __float2bfloat16_rn(v); }
   __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
     return fmaf(__bfloat162float(v), corr, wf_of(d) * (corr - 1.0f));
@@ -151,6 +167,11 @@ struct Layout {
     const long long r = cell / nx;
     return r * pitch + (cell - r * nx);
   }
+  // the same two by x-row (iy + ny * iz) and x
+  __host__ __device__ long long at_row(int d, long long row, int x) const {
+    return row * rstride + (long long)slot(d) * dstride + x;
+  }
+  __host__ __device__ long long cls_at_row(long long row, int x) const { return row * pitch + x; }
 };
 
 __host__ inline Layout make_layout(int nx, int ny, int nz) {

@@ -57,7 +57,12 @@ struct aerosim_engine {
   unsigned long long* stats_buf = nullptr;
   void* staging = nullptr;
   size_t staging_bytes = 0;
-  double* frame_host = nullptr;  // pinned: force sums [8] and the device error flag of a frame
+  // pinned and mapped into the device's address space, written by the kernels directly
+  double* frame_host = nullptr;  // force sums [8] and the device error flag of a frame
+  double* frame_dev = nullptr;   // its device address
+  uint8_t* slice_host = nullptr;  // pinned, not mapped: the slice image on its way to the caller
+  size_t slice_host_bytes = 0;
+  size_t slice_bytes = 0;         // size of the last enqueued slice image
   long long step_index = 0;
   double last_ms = 0;
   long long last_launches = 0;
@@ -437,6 +442,7 @@ int aerosim_destroy(aerosim_engine* h) {
   cudaFree(h->force_partials); cudaFree(h->force_ticket); cudaFree(h->force_out);
   cudaFree(h->stats_buf); cudaFree(h->staging);
   if (h->frame_host) cudaFreeHost(h->frame_host);
+  if (h->slice_host) cudaFreeHost(h->slice_host);
   cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -659,16 +665,28 @@ int finish_steps(aerosim_engine* h, int dev_err) {
 
 // Enqueues the momentum-exchange reduction of the current populations; its eight FP64
 // sums land in `dst` (device-to-host, asynchronous when dst is pinned).
-int enqueue_forces(aerosim_engine* h, double* dst) {
+// With dst_dev (the device address of mapped pinned memory at dst) the kernel writes
+// the sums, and err_dev the steps' error code, to the host directly.
+int enqueue_forces(aerosim_engine* h, double* dst, double* dst_dev = nullptr, int* err_dev = nullptr) {
   ForceArgs a{};
   a.f = h->f[h->cur];
   a.cls = h->g.cls; a.bcells = h->g.bcells; a.q = h->g.q; a.st = h->st;
-  a.partials = h->force_partials; a.ticket = h->force_ticket; a.out = h->force_out;
+  a.partials = h->force_partials; a.ticket = h->force_ticket;
+  a.out = dst_dev ? dst_dev : h->force_out;
+  a.err_out = err_dev;
   a.L = h->L; a.B = h->g.B;
   a.prev_slot = prev_slot(h);
   const unsigned grid = (unsigned)std::min<long long>((h->g.B + 7) / 8, h->force_blocks_cap);
   CU(h, launch_forces(h->cfg.precision, a, grid, h->stream));
-  CU(h, cudaMemcpyAsync(dst, h->force_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (!dst_dev) CU(h, cudaMemcpyAsync(dst, h->force_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return AEROSIM_OK;
+}
+
+// The engine's mapped pinned frame buffer (force sums and error code).
+int ensure_frame_host(aerosim_engine* h) {
+  if (h->frame_host) return AEROSIM_OK;
+  CU(h, cudaHostAlloc((void**)&h->frame_host, 16 * sizeof(double), cudaHostAllocMapped));
+  CU(h, cudaHostGetDevicePointer((void**)&h->frame_dev, h->frame_host, 0));
   return AEROSIM_OK;
 }
 
@@ -707,9 +725,10 @@ int aerosim_read_forces(aerosim_engine* h, aerosim_forces* out) {
   CU(h, cudaSetDevice(h->device));
   double r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (h->g.B > 0) {
-    int rc = enqueue_forces(h, r);
-    if (rc) return rc;
+    int rc = ensure_frame_host(h);
+    if (rc || (rc = enqueue_forces(h, h->frame_host, h->frame_dev))) return rc;
     CU(h, cudaStreamSynchronize(h->stream));
+    std::memcpy(r, h->frame_host, sizeof(r));
   }
   forces_from_sums(h, r, out);
   return AEROSIM_OK;
@@ -897,9 +916,20 @@ int enqueue_slice(aerosim_engine* h, int32_t axis, double fraction, int32_t mode
   const size_t bytes = (size_t)w * hh * 4;
   int rc = ensure_staging(h, bytes);
   if (rc) return rc;
+  if (bytes > h->slice_host_bytes) {
+    if (h->slice_host) cudaFreeHost(h->slice_host);
+    h->slice_host = nullptr;
+    h->slice_host_bytes = 0;
+    CU(h, cudaHostAlloc((void**)&h->slice_host, bytes, cudaHostAllocDefault));
+    h->slice_host_bytes = bytes;
+  }
   CU(h, launch_slice(h->mux, h->muy, h->muz, h->mrho, h->g.cls, h->st, prev_slot(h), h->L, axis, fixed, mode,
                      js_max(1e-4, h->cfg.u_inlet_lattice), w, hh, static_cast<uint8_t*>(h->staging), h->stream));
-  CU(h, cudaMemcpyAsync(rgba, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+  // into pinned memory inside the stream (no host round trip of a pageable copy; the
+  // kernel's own byte stores to mapped host memory measured slower); the caller copies
+  // it into its buffer once the stream has drained
+  CU(h, cudaMemcpyAsync(h->slice_host, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+  h->slice_bytes = bytes;
   return AEROSIM_OK;
 }
 
@@ -911,6 +941,7 @@ extern "C" int aerosim_extract_slice(aerosim_engine* h, int32_t axis, double fra
   int rc = enqueue_slice(h, axis, fraction, mode, rgba, width, height);
   if (rc || !rgba) return rc;
   CU(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(rgba, h->slice_host, h->slice_bytes);
   return AEROSIM_OK;
 }
 
@@ -924,17 +955,21 @@ extern "C" int aerosim_step_and_extract_slice(aerosim_engine* h, int32_t n, int3
   if (!h || !forces || (rgba && (!width || !height))) return AEROSIM_ERR_ARG;
   if (!h->have_grid || !h->f[0]) return fail(h, AEROSIM_ERR_STATE, "step_and_extract_slice: no voxel grid");
   CU(h, cudaSetDevice(h->device));
-  if (!h->frame_host) CU(h, cudaHostAlloc((void**)&h->frame_host, 16 * sizeof(double), cudaHostAllocDefault));
+  int rc = ensure_frame_host(h);
+  if (rc) return rc;
   double* sums = h->frame_host;
   int* dev_err = reinterpret_cast<int*>(h->frame_host + 8);
   *dev_err = 0;
   for (int i = 0; i < 8; ++i) sums[i] = 0.0;
-  int rc = enqueue_steps(h, n);
-  if (rc) return rc;
-  CU(h, cudaMemcpyAsync(dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  if (h->g.B > 0 && (rc = enqueue_forces(h, sums))) return rc;
+  if ((rc = enqueue_steps(h, n))) return rc;
+  if (h->g.B > 0) {  // the force kernel's last CTA writes the sums and the error code
+    if ((rc = enqueue_forces(h, sums, h->frame_dev, reinterpret_cast<int*>(h->frame_dev + 8)))) return rc;
+  } else {
+    CU(h, cudaMemcpyAsync(dev_err, &h->st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  }
   if (rgba && (rc = enqueue_slice(h, axis, fraction, mode, rgba, width, height))) return rc;
   CU(h, cudaStreamSynchronize(h->stream));
+  if (rgba) std::memcpy(rgba, h->slice_host, h->slice_bytes);
   if ((rc = finish_steps(h, *dev_err))) return rc;
   forces_from_sums(h, sums, forces);
   return AEROSIM_OK;

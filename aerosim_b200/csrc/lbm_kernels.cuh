@@ -88,6 +88,7 @@ struct ForceArgs {
   double* partials;       // [gridDim.x * 8]
   unsigned int* ticket;
   double* out;            // [8]: fx fy fz mx my mz cut_face_links blocks
+  int* err_out;           // receives the steps' error code, or null
   Layout L;
   long long B;
   int prev_slot;          // state slot of the step that produced f (-1: none)
@@ -319,7 +320,7 @@ struct MlpRefs {
 
 template <class S, bool MLP = false>
 __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux, float& uy, float& uz,
-                                             float tau0, float k_smag, const MlpRefs* m = nullptr) {
+                                             float tau0, float k_smag, float2 dec, const MlpRefs* m = nullptr) {
   constexpr float OS = S::kOutScale, OW = S::kOutW;
   constexpr float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
   float s[9], t[9];
@@ -328,14 +329,24 @@ __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux
     s[p] = h[2 * p + 1] + h[2 * p + 2];
     t[p] = h[2 * p + 1] - h[2 * p + 2];
   }
-  const float dr = h[0] + ((s[0] + s[1]) + (s[2] + s[3]) + ((s[4] + s[5]) + (s[6] + s[7])) + s[8]);
-  const float jx = (t[0] + t[3]) + (t[4] + t[5]) + t[6];
-  const float jy = (t[1] + t[3]) - t[4] + (t[7] + t[8]);
-  const float jz = (t[2] + t[5]) - t[6] + (t[7] - t[8]);
-  const float sxx = (s[0] + s[3]) + (s[4] + s[5]) + s[6];
-  const float syy = (s[1] + s[3]) + (s[4] + s[7]) + s[8];
-  const float szz = (s[2] + s[5]) + (s[6] + s[7]) + s[8];
-  const float sxy = s[3] - s[4], sxz = s[5] - s[6], syz = s[7] - s[8];
+  float dr = h[0] + ((s[0] + s[1]) + (s[2] + s[3]) + ((s[4] + s[5]) + (s[6] + s[7])) + s[8]);
+  float jx = (t[0] + t[3]) + (t[4] + t[5]) + t[6];
+  float jy = (t[1] + t[3]) - t[4] + (t[7] + t[8]);
+  float jz = (t[2] + t[5]) - t[6] + (t[7] - t[8]);
+  float sxx = (s[0] + s[3]) + (s[4] + s[5]) + s[6];
+  float syy = (s[1] + s[3]) + (s[4] + s[7]) + s[8];
+  float szz = (s[2] + s[5]) + (s[6] + s[7]) + s[8];
+  float sxy = s[3] - s[4], sxz = s[5] - s[6], syz = s[7] - s[8];
+  if constexpr (S::kRawMoments) {
+    // h holds raw stored values, h_i = dec.x raw_i + dec.y w_i (dec = storage scale x
+    // pending rescale, rescale - 1): with sum w = 1, sum w c = 0, sum w c_a c_a = 1/3
+    // and sum w c_a c_b = 0 the ten moments take the decode in ten operations
+    const float cw3 = dec.y * (1.0f / 3.0f);
+    dr = fmaf(dr, dec.x, dec.y);
+    jx *= dec.x; jy *= dec.x; jz *= dec.x;
+    sxx = fmaf(sxx, dec.x, cw3); syy = fmaf(syy, dec.x, cw3); szz = fmaf(szz, dec.x, cw3);
+    sxy *= dec.x; sxz *= dec.x; syz *= dec.x;
+  }
 
   r = fmaxf(0.5f, fminf(1.8f, 1.0f + dr));
   if (dr != dr) r = dr;  // keep NaN visible like Math.min / Math.max
@@ -786,7 +797,8 @@ struct SegGeom {
 
 template <class S, class InletFn, bool MLP = false>
 __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __restrict__ fd, const SegGeom g,
-                                             float tau0, float k_smag, InletFn inlet_u, const StepArgs& m,
+                                             float tau0, float k_smag, float2 dec, InletFn inlet_u,
+                                             const StepArgs& m,
                                              float* xo, const float4* s_dcw, const int* s_dslot, int lane,
                                              long long& my_sum, int& my_nan, const MlpRefs* mlp = nullptr) {
   using T = typename S::T;
@@ -798,9 +810,9 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
   if constexpr (MLP) {
     MlpRefs mr = *mlp;
     mr.wall_dist = (float)(g.cl >> 3);
-    collide_fast<S, true>(v, r, ux, uy, uz, tau0, k_smag, &mr);  // v: storage domain
+    collide_fast<S, true>(v, r, ux, uy, uz, tau0, k_smag, dec, &mr);  // v: storage domain
   } else {
-    collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag);
+    collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag, dec);
   }
   if (g.row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
     // inlet (:328-352): density of ix = 1 (1 for a solid, :177); a near-wall ix = 1
@@ -1055,6 +1067,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     const double corr = a.st->apply[pslot] ? a.st->corr[pslot] : 1.0;
     const float corrf = (float)corr;
     const float corrf_s = corrf * F16S_INV_SCALE;
+    const float2 dec = make_float2(corrf * S::kRawScale, corrf - 1.0f);  // raw-moment decode
     const int ry = warp / wpr;
     const int nchunks = (nx + shift + span - 1) / span;
     int my_nan = 0;
@@ -1096,7 +1109,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
 #pragma unroll
           for (int d = 0; d < 19; ++d) {
             const T raw = sp[slot_of(d) * pitch + lx - cx_of(d)];
-            if constexpr (MODE == MODE_FAST) v[d] = S::h_scaled(raw, d, corrf, corrf_s);
+            if constexpr (MODE == MODE_FAST && S::kRawMoments) v[d] = S::raw(raw);
+            else if constexpr (MODE == MODE_FAST) v[d] = S::h_scaled(raw, d, corrf, corrf_s);
             else if constexpr (MODE == MODE_MIRROR) v[d] = (double)(float)(S::f_of(raw, d) * corr);
             else v[d] = S::f_of(raw, d) * corr;
           }
@@ -1114,10 +1128,11 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
             auto inlet = [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); };
             if constexpr (MLP) {
               const MlpRefs mr{s_mfrag, s_mbias, s_mstage + warp * 128, a.mlp_nu0, 0.0f, lane};
-              fast_segment<S, decltype(inlet), true>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a,
+              fast_segment<S, decltype(inlet), true>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a,
                                                      s_xo + warp * 20, s_dcw, s_dslot, lane, my_sum, my_nan, &mr);
             } else {
-              fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, inlet, a, s_xo + warp * 20, s_dcw, s_dslot,
+              fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a, s_xo + warp * 20, s_dcw,
+                              s_dslot,
                               lane, my_sum, my_nan);
             }
           } else {
@@ -1189,8 +1204,8 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int apply = a.prev_slot >= 0 ? a.st->apply[a.prev_slot] : 0;
   const double corr = apply ? a.st->corr[a.prev_slot] : 1.0;
-  auto pop = [&](int d, long long i) -> double {
-    const double v = S::f_of(f[a.L.at(d, i)], d);
+  auto pop = [&](int d, long long row, int x) -> double {
+    const double v = S::f_of(f[a.L.at_row(d, row, x)], d);
     if constexpr (MODE == MODE_MIRROR) return (double)(float)(v * corr);
     else return v * corr;
   };
@@ -1207,27 +1222,27 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long b = (long long)blockIdx.x * (blockDim.x >> 5) + warp; b < a.B; b += warps) {
-    const long long ci = a.bcells[b];
-    const int ix = (int)(ci % nx);
-    const long long rem = (ci - ix) / nx;
-    const int iy = (int)(rem % ny);
-    const int iz = (int)((rem - iy) / ny);
+    const int ci = a.bcells[b];  // cell indices are int32 in the voxel grid
+    const int row = ci / nx;      // iy + ny * iz
+    const int ix = ci - row * nx;
+    const int iz = row / ny;
+    const int iy = row - iz * ny;
     double cfx = 0.0, cfy = 0.0, cfz = 0.0, cut = 0.0;
     if (lane < 18) {
       const double qv = (double)a.q[b * 18 + lane];
       if (qv > 0.0) {
-        const double fo = pop(d, ci);
+        const double fo = pop(d, row, ix);
         const int ax = clampi(ix - cx, 0, nx - 1);  // cell + c_opp(d)
         const int ay = clampi(iy - cy, 0, ny - 1);
         const int az = clampi(iz - cz, 0, nz - 1);
-        const long long ff = ax + (long long)nx * (ay + (long long)ny * az);
+        const long long frow = ay + (long long)ny * az;
         double fi = fo;
-        if ((a.cls[a.L.cls_at(ff)] & CLS_FLAG_MASK) != 1) {
+        if ((a.cls[a.L.cls_at_row(frow, ax)] & CLS_FLAG_MASK) != 1) {
           if (qv < 0.5) {
-            const double fon = pop(d, ff);
+            const double fon = pop(d, frow, ax);
             fi = 2.0 * qv * fo + (1.0 - 2.0 * qv) * fon;
           } else {
-            const double fic = pop(od, ci);
+            const double fic = pop(od, row, ix);
             const double inv2q = 1.0 / (2.0 * qv);
             fi = inv2q * fo + (1.0 - inv2q) * fic;
           }
@@ -1274,19 +1289,30 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
   }
   __syncthreads();
   if (is_last) {
-    // component k by warp k: lanes stride over the CTAs' partials, then a shuffle tree
-    // (a fixed order, so the total does not depend on which CTA finished last)
+    // every thread adds a fixed stride of the CTAs' partials (its loads in flight
+    // together), then shuffle trees and the warps in order: a fixed order, so the total
+    // does not depend on which CTA finished last
     __threadfence();
-    if (warp < 7) {
-      double s = 0.0;
-      for (unsigned int blk = lane; blk < gridDim.x; blk += 32)
-        s += __ldcg(&a.partials[(long long)blk * 8 + warp]);
+    double s[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (unsigned int blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x) {
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (lane == 0) a.out[warp] = s;
+      for (int k = 0; k < 7; ++k) s[k] += __ldcg(&a.partials[(long long)blk * 8 + k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_down_sync(0xffffffffu, s[k], o);
+      if (lane == 0) red[warp][k] = s[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+      a.out[threadIdx.x] = t;
     }
     if (threadIdx.x == 0) {
       a.out[7] = (double)gridDim.x;
+      if (a.err_out) *a.err_out = a.st->error;
       *a.ticket = 0u;
     }
   }

@@ -173,6 +173,7 @@ class LBMEngine:
         self.config = _default_config()
         self.voxel: VoxelGridResult | None = None
         self._has_grid = False
+        self._slice_dims: dict = {}  # axis -> (width, height) of the current grid's slices
         self.force_tracker = ForceConvergenceTracker()
 
     # -- configuration ----------------------------------------------------
@@ -208,6 +209,7 @@ class LBMEngine:
                      N.ptr(origin, C.c_double), N.ptr(flags, C.c_uint8), N.ptr(bmap, C.c_int32),
                      N.ptr(bcells, C.c_int32), N.ptr(q, C.c_float), int(bcells.size), 1 if reset_flow else 0)
         self._has_grid = True
+        self._slice_dims = {}
 
     def voxelize(self, geometry, world_matrix, tunnel, grid, config: dict | None = None,
                  reset_flow: bool = True) -> N.VoxelInfo:
@@ -220,6 +222,7 @@ class LBMEngine:
         info = voxelize_into(self._h, geometry, world_matrix, tunnel, grid, reset_flow)
         self.voxel = None
         self._has_grid = True
+        self._slice_dims = {}
         return info
 
     def read_voxel_grid(self) -> VoxelGridResult:
@@ -309,8 +312,11 @@ class LBMEngine:
             a = {"x": 0, "y": 1, "z": 2}[slice.get("axis", "z")]
             m = {"velocity": 0, "vorticity": 1, "pressure": 2}[slice.get("mode", "velocity")]
             frac = float(slice.get("fraction", 0.5))
-            self._h.call("aerosim_extract_slice", a, frac, m, None, C.byref(w), C.byref(h))
-            rgba = np.empty(w.value * h.value * 4, np.uint8)
+            dims = self._slice_dims.get(a)
+            if dims is None:  # the image size of this axis, asked once per grid
+                self._h.call("aerosim_extract_slice", a, frac, m, None, C.byref(w), C.byref(h))
+                dims = self._slice_dims[a] = (w.value, h.value)
+            rgba = np.empty(dims[0] * dims[1] * 4, np.uint8)
             self._h.call("aerosim_step_and_extract_slice", int(substeps), a, frac, m, N.ptr(rgba, C.c_uint8),
                          C.byref(w), C.byref(h), C.byref(f))
         c = self.config
