@@ -996,6 +996,13 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     s_uyi[i] = uyi;
   }
   __syncthreads();
+  // Programmatic dependent launch: this CTA may have started while the previous kernel
+  // of the stream was still finishing.  Everything above wrote only shared memory and
+  // read only inputs the host copied in; wait for that kernel to complete and flush
+  // before reading its results or overwriting what it reads.  Then let the next step's
+  // CTAs be scheduled as this grid's CTAs exit (all of this grid is resident already).
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   long long my_sum = 0;
   bool failed = false;

@@ -34,9 +34,21 @@ cudaError_t step_entry(const StepArgs& a, dim3 block, unsigned grid, size_t smem
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, (int)(block.x * block.y), smem);
   }
-  k<<<grid, block, smem, s>>>(a);
+  // programmatic dependent launch: the CTAs of a step may start (and run their
+  // shared-memory prologue) while the previous step's last CTAs finish
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k, a);
   if (launches) *launches = 1;
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 // The FP32-arithmetic kernels are compiled for every row pitch up to 256 (multiples
