@@ -51,7 +51,7 @@ __host__ __device__ inline double js_max(double a, double b) {
 constexpr float F16S_SCALE = 32768.0f;
 constexpr float F16S_INV_SCALE = 1.0f / 32768.0f;
 
-// Population storage codecs.  All four expose the same interface in terms of the
+// Population storage codecs.  All five expose the same interface in terms of the
 // deviation h = f - w_d from the rest weight (the form the FP32 collision works in)
 // and of the full value f (the form the FP64 paths work in):
 //   h_of(raw, d), raw_of_h(h, d)  -- float deviation
@@ -78,6 +78,25 @@ struct StoreF32 {
   __device__ __forceinline__ static T raw_of_h(float h, int d) { return wf_of(d) + h; }
   __device__ __forceinline__ static double f_of(T v, int) { return (double)v; }
   __device__ __forceinline__ static T raw_of_f(double f, int) { return (float)f; }
+};
+// FP32 storage of the deviation f - w_d, for the FP32-arithmetic kernels: the collision
+// takes the stored deviations as they are and decodes its ten moments (kRawMoments), and
+// the deviations keep float's full relative precision (storing f = w_d + h rounds h to
+// the ulp of w_d).  The bit-parity mode keeps StoreF32, the reference's own values.
+struct StoreF32S {
+  using T = float;
+  static constexpr float kOutScale = 1.0f, kOutW = 0.0f;
+  static constexpr bool kRawMoments = true;
+  static constexpr float kRawScale = 1.0f;
+  __device__ __forceinline__ static float raw(T v) { return v; }
+  __device__ __forceinline__ static T store(float v) { return v; }
+  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
+    return fmaf(v, corr, wf_of(d) * (corr - 1.0f));
+  }
+  __device__ __forceinline__ static float h_of(T v, int) { return v; }
+  __device__ __forceinline__ static T raw_of_h(float h, int) { return h; }
+  __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)v; }
+  __device__ __forceinline__ static T raw_of_f(double f, int d) { return (float)(f - (double)wf_of(d)); }
 };
 struct StoreF64 {
   using T = double;

@@ -34,7 +34,7 @@ cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned g
 
 cudaError_t launch_forces(int precision, const ForceArgs& a, unsigned grid, cudaStream_t s) {
   switch (precision) {
-    case AEROSIM_PREC_F32: forces_kernel<StoreF32, MODE_FAST><<<grid, 256, 0, s>>>(a); break;
+    case AEROSIM_PREC_F32: forces_kernel<StoreF32S, MODE_FAST><<<grid, 256, 0, s>>>(a); break;
     case AEROSIM_PREC_F32_MIRROR: forces_kernel<StoreF32, MODE_MIRROR><<<grid, 256, 0, s>>>(a); break;
     case AEROSIM_PREC_F16S: forces_kernel<StoreF16S, MODE_FAST><<<grid, 256, 0, s>>>(a); break;
     case AEROSIM_PREC_BF16S: forces_kernel<StoreBF16S, MODE_FAST><<<grid, 256, 0, s>>>(a); break;
@@ -61,7 +61,8 @@ cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, f
   const unsigned g = grid_for((long long)L.nx * L.ny * L.nz);
 #define AEROSIM_INIT(S) init_kernel<S><<<g, 256, 0, s>>>(f0, f1, cls, mux, muy, muz, mrho, abl, L, u_inlet, gns)
   switch (precision) {
-    case AEROSIM_PREC_F32: case AEROSIM_PREC_F32_MIRROR: AEROSIM_INIT(StoreF32); break;
+    case AEROSIM_PREC_F32: AEROSIM_INIT(StoreF32S); break;
+    case AEROSIM_PREC_F32_MIRROR: AEROSIM_INIT(StoreF32); break;
     case AEROSIM_PREC_F16S: AEROSIM_INIT(StoreF16S); break;
     case AEROSIM_PREC_BF16S: AEROSIM_INIT(StoreBF16S); break;
     case AEROSIM_PREC_F64: AEROSIM_INIT(StoreF64); break;
@@ -83,7 +84,7 @@ static void read_pops_t(const void* f, const uint8_t* cls, const StepState* st, 
 cudaError_t launch_read_pops(int precision, const void* f, const uint8_t* cls, const StepState* st,
                              int ps, const Layout& L, long long N, void* out, int dtype, cudaStream_t s) {
   switch (precision) {
-    case AEROSIM_PREC_F32: read_pops_t<StoreF32, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
+    case AEROSIM_PREC_F32: read_pops_t<StoreF32S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
     case AEROSIM_PREC_F32_MIRROR: read_pops_t<StoreF32, MODE_MIRROR>(f, cls, st, ps, L, N, out, dtype, s); break;
     case AEROSIM_PREC_F16S: read_pops_t<StoreF16S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
     case AEROSIM_PREC_BF16S: read_pops_t<StoreBF16S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
@@ -104,7 +105,8 @@ static void write_pops_t(void* f, const Layout& L, long long N, const void* in, 
 cudaError_t launch_write_pops(int precision, void* f, const Layout& L, long long N, const void* in,
                               int dtype, cudaStream_t s) {
   switch (precision) {
-    case AEROSIM_PREC_F32: case AEROSIM_PREC_F32_MIRROR: write_pops_t<StoreF32>(f, L, N, in, dtype, s); break;
+    case AEROSIM_PREC_F32: write_pops_t<StoreF32S>(f, L, N, in, dtype, s); break;
+    case AEROSIM_PREC_F32_MIRROR: write_pops_t<StoreF32>(f, L, N, in, dtype, s); break;
     case AEROSIM_PREC_F16S: write_pops_t<StoreF16S>(f, L, N, in, dtype, s); break;
     case AEROSIM_PREC_BF16S: write_pops_t<StoreBF16S>(f, L, N, in, dtype, s); break;
     case AEROSIM_PREC_F64: write_pops_t<StoreF64>(f, L, N, in, dtype, s); break;
@@ -117,7 +119,7 @@ cudaError_t launch_materialize(int precision, void* f, const uint8_t* cls, const
                                const Layout& L, long long N, cudaStream_t s) {
   const unsigned g = grid_for(N);
   switch (precision) {
-    case AEROSIM_PREC_F32: materialize_rescale_kernel<StoreF32, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
+    case AEROSIM_PREC_F32: materialize_rescale_kernel<StoreF32S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     case AEROSIM_PREC_F32_MIRROR: materialize_rescale_kernel<StoreF32, MODE_MIRROR><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     case AEROSIM_PREC_F16S: materialize_rescale_kernel<StoreF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     case AEROSIM_PREC_BF16S: materialize_rescale_kernel<StoreBF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;

@@ -44,8 +44,8 @@ enum aerosim_cell_flag { AEROSIM_CELL_FLUID = 0, AEROSIM_CELL_SOLID = 1, AEROSIM
 
 /* Population storage / arithmetic of the solver. */
 enum aerosim_precision {
-  AEROSIM_PREC_F32 = 0,        /* FP32 storage, FP32 collision (the production path) */
-  AEROSIM_PREC_F32_MIRROR = 1, /* FP32 storage, FP64 arithmetic rounded exactly like the
+  AEROSIM_PREC_F32 = 0,        /* FP32 storage of (f - w), FP32 collision (the production path) */
+  AEROSIM_PREC_F32_MIRROR = 1, /* FP32 storage of f, FP64 arithmetic rounded exactly like the
                                   reference's JavaScript CPU solver (bit-parity mode) */
   AEROSIM_PREC_F16S = 2,       /* FP16 storage of (f - w) scaled by 2^15, FP32 collision */
   AEROSIM_PREC_BF16S = 3,      /* BF16 storage of (f - w), FP32 collision */
