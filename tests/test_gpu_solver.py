@@ -208,6 +208,26 @@ def test_error_status_paths(gpu_engine_cls):
     assert eng.step_and_extract_slice(4) is None
 
 
+def test_fused_frame_without_boundary_cells(gpu_engine_cls, oracle_mod):
+    """An empty tunnel has no boundary cells, so no force kernel runs in the frame and the
+    steps' error code comes back by its own copy: zero forces, the step count advancing,
+    the image of a split call, and the same populations as plain steps on a twin."""
+    case = cases.Case("empty", 40, 16, 16, (np.zeros((0, 3), np.float32), None), 0.05, 0.01, 0.1, 8)
+    _, _, fused = _pair(gpu_engine_cls, oracle_mod, case, "f32")
+    _, _, split = _pair(gpu_engine_cls, oracle_mod, case, "f32")
+    for k in range(3):
+        a = fused.step_and_extract_slice(4, slice={"axis": "z", "fraction": 0.5, "mode": "velocity"})
+        split.step(4)
+        f = a["forces"]
+        assert (f.fx, f.fy, f.fz, f.mz, f.cut_face_links) == (0.0, 0.0, 0.0, 0.0, 0)
+        assert a["stepCount"] == 4 * (k + 1)
+        b = split.extract_slice_rgba("z", 0.5, "velocity")
+        assert (a["width"], a["height"]) == (40, 16) and np.array_equal(a["rgba"], b["rgba"])
+    assert np.array_equal(fused.read_populations().view(np.uint32), split.read_populations().view(np.uint32))
+    fused.close()
+    split.close()
+
+
 @pytest.mark.parametrize("dims", [(33, 12, 10), (97, 9, 7), (289, 6, 6), (3, 5, 6), (40, 20, 3), (64, 1, 8),
                                   (65, 10, 8), (150, 8, 6), (200, 6, 6)])
 def test_mirror_bit_exact_awkward_lattices(gpu_engine_cls, oracle_mod, dims):
