@@ -57,23 +57,19 @@ constexpr float F16S_INV_SCALE = 1.0f / 32768.0f;
 //   h_of(raw, d), raw_of_h(h, d)  -- float deviation
 //   f_of(raw, d), raw_of_f(f, d)  -- double value
 // d is a loop index of fully unrolled loops, so w_d folds to a constant.
-// h_scaled(raw, d, corr, corr_s) returns f * corr - w_d in one fused step (the
-// pending mean-density rescale folded into the load; corr_s = corr / 2^15).
+// kRawMoments marks the codecs of stored deviations, the ones the FP32-arithmetic
+// kernels run on: those take the stored values as they are (raw()) and apply the storage
+// scale kRawScale and the pending mean-density rescale to the collision's ten moments
+// instead of to the 19 values (a full f would lose its small moments to cancellation
+// against the rest weights).
 struct StoreF32 {
   using T = float;
   // FP32-collision output in the storage domain: value = kOutScale * h + kOutW * w_d
   static constexpr float kOutScale = 1.0f, kOutW = 1.0f;
-  // kRawMoments: the collision takes the stored values as they are (raw()) and applies
-  // the storage scale kRawScale and the pending rescale to its ten moments instead of
-  // to the 19 values (stored deviations only: a full f would lose its small moments
-  // to cancellation against the rest weights)
   static constexpr bool kRawMoments = false;
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return v; }
   __device__ __forceinline__ static T store(float v) { return v; }
-  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
-    return fmaf(v, corr, -wf_of(d));
-  }
   __device__ __forceinline__ static float h_of(T v, int d) { return v - wf_of(d); }
   __device__ __forceinline__ static T raw_of_h(float h, int d) { return wf_of(d) + h; }
   __device__ __forceinline__ static double f_of(T v, int) { return (double)v; }
@@ -90,9 +86,6 @@ struct StoreF32S {
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return v; }
   __device__ __forceinline__ static T store(float v) { return v; }
-  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
-    return fmaf(v, corr, wf_of(d) * (corr - 1.0f));
-  }
   __device__ __forceinline__ static float h_of(T v, int) { return v; }
   __device__ __forceinline__ static T raw_of_h(float h, int) { return h; }
   __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)v; }
@@ -105,9 +98,6 @@ struct StoreF64 {
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return (float)v; }
   __device__ __forceinline__ static T store(float v) { return (double)v; }
-  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
-    return (float)(v * (double)corr - w64_of(d));
-  }
   __device__ __forceinline__ static float h_of(T v, int d) { return (float)(v - w64_of(d)); }
   __device__ __forceinline__ static T raw_of_h(float h, int d) { return w64_of(d) + (double)h; }
   __device__ __forceinline__ static double f_of(T v, int) { return v; }
@@ -120,9 +110,6 @@ struct StoreF16S {
   static constexpr float kRawScale = F16S_INV_SCALE;
   __device__ __forceinline__ static float raw(T v) { return __half2float(v); }
   __device__ __forceinline__ static T store(float v) { return __float2half_rn(v); }
-  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float corr_s) {
-    return fmaf(__half2float(v), corr_s, wf_of(d) * (corr - 1.0f));
-  }
   __device__ __forceinline__ static float h_of(T v, int) { return __half2float(v) * F16S_INV_SCALE; }
   __device__ __forceinline__ static T raw_of_h(float h, int) { return __float2half_rn(h * F16S_SCALE); }
   __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)h_of(v, d); }
@@ -135,9 +122,6 @@ struct StoreBF16S {
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return __bfloat162float(v); }
   __device__ __forceinline__ static T store(float v) { return __float2bfloat16_rn(v); }
-  __device__ __forceinline__ static float h_scaled(T v, int d, float corr, float) {
-    return fmaf(__bfloat162float(v), corr, wf_of(d) * (corr - 1.0f));
-  }
   __device__ __forceinline__ static float h_of(T v, int) { return __bfloat162float(v); }
   __device__ __forceinline__ static T raw_of_h(float h, int) { return __float2bfloat16_rn(h); }
   __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)h_of(v, d); }

@@ -228,7 +228,6 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
       }
       const double corr = ia.st->apply[pslot] ? ia.st->corr[pslot] : 1.0;
       const float corrf = (float)corr;
-      const float corrf_s = corrf * F16S_INV_SCALE;
       const float2 dec = make_float2(corrf * S::kRawScale, corrf - 1.0f);  // raw-moment decode
       const float tau0f = (float)ia.tau0, ksmagf = (float)ia.k_smag;
       T* fd = static_cast<T*>(b.bufs[2 * k + (cur ^ 1)]);
@@ -247,11 +246,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
         const uint8_t cl = sc[lx];
         float v[19];
 #pragma unroll
-        for (int d = 0; d < 19; ++d) {
-          const T raw = sp[slot_of(d) * pitch + lx - cx_of(d)];
-          if constexpr (S::kRawMoments) v[d] = S::raw(raw);
-          else v[d] = S::h_scaled(raw, d, corrf, corrf_s);
-        }
+        for (int d = 0; d < 19; ++d) v[d] = S::raw(sp[slot_of(d) * pitch + lx - cx_of(d)]);  // decoded in the moments
         if (sg + kConsumerWarps >= total) {  // this warp's last segment of the slot
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[s]);

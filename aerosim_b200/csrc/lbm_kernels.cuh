@@ -321,6 +321,7 @@ struct MlpRefs {
 template <class S, bool MLP = false>
 __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux, float& uy, float& uz,
                                              float tau0, float k_smag, float2 dec, const MlpRefs* m = nullptr) {
+  static_assert(S::kRawMoments, "the FP32 collision runs on stored deviations");
   constexpr float OS = S::kOutScale, OW = S::kOutW;
   constexpr float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
   float s[9], t[9];
@@ -337,7 +338,7 @@ __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux
   float syy = (s[1] + s[3]) + (s[4] + s[7]) + s[8];
   float szz = (s[2] + s[5]) + (s[6] + s[7]) + s[8];
   float sxy = s[3] - s[4], sxz = s[5] - s[6], syz = s[7] - s[8];
-  if constexpr (S::kRawMoments) {
+  {
     // h holds raw stored values, h_i = dec.x raw_i + dec.y w_i (dec = storage scale x
     // pending rescale, rescale - 1): with sum w = 1, sum w c = 0, sum w c_a c_a = 1/3
     // and sum w c_a c_b = 0 the ten moments take the decode in ten operations
@@ -1073,7 +1074,6 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     const int pslot = (a.step_index + 1) & 1;  // pending rescale of the previous step
     const double corr = a.st->apply[pslot] ? a.st->corr[pslot] : 1.0;
     const float corrf = (float)corr;
-    const float corrf_s = corrf * F16S_INV_SCALE;
     const float2 dec = make_float2(corrf * S::kRawScale, corrf - 1.0f);  // raw-moment decode
     const int ry = warp / wpr;
     const int nchunks = (nx + shift + span - 1) / span;
@@ -1116,8 +1116,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
 #pragma unroll
           for (int d = 0; d < 19; ++d) {
             const T raw = sp[slot_of(d) * pitch + lx - cx_of(d)];
-            if constexpr (MODE == MODE_FAST && S::kRawMoments) v[d] = S::raw(raw);
-            else if constexpr (MODE == MODE_FAST) v[d] = S::h_scaled(raw, d, corrf, corrf_s);
+            if constexpr (MODE == MODE_FAST) v[d] = S::raw(raw);  // decoded in the moments
             else if constexpr (MODE == MODE_MIRROR) v[d] = (double)(float)(S::f_of(raw, d) * corr);
             else v[d] = S::f_of(raw, d) * corr;
           }
