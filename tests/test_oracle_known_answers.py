@@ -10,6 +10,8 @@ answers the reference's test suite asserts:
   phase3.test.ts:8-43     Re = 1e5 mass conservation, 10 000 steps
   phase3.test.ts:45-124   Karman street Strouhal number
   phase4.test.ts:119-159  Cd bands of the calibration bodies (testRunner.ts:39-155)
+  phase5.test.ts:86-116   vortex cores (Q > 0) in the wake of a cube
+  phase5.test.ts:120-177  stagnation Cp near +1 in front of a cube, suction in its wake
 The meshes are this project's generators standing in for the three.js presets.
 """
 import math
@@ -249,3 +251,43 @@ def test_q_criterion_known_answers():
     assert abs(r["omegaMag"][mid] - 10.0) < 0.5
     s = oracle.q_criterion(nx, ny, nz, dx, *[a.astype(np.float32).ravel() for a in shear])
     assert abs(s["qValues"][mid]) < 1e-4
+
+
+def _scaled(k):
+    """A world matrix (column-major, like three.js Matrix4.elements) scaling by k."""
+    return [k, 0, 0, 0, 0, k, 0, 0, 0, 0, k, 0, 0, 0, 0, 1]
+
+
+def test_wake_vortex_cores(oracle_mod):
+    """phase5.test.ts:86-116: the 'cube' preset scaled by 0.4 in a 3 x 1.5 x 1.5 m
+    tunnel on 36x18x18, u = 0.085, nu = 0.005, Cs = 0.12, 80 steps from the impulsive
+    start: the Q-criterion finds vortex cores (max Q > 1e-4) and max |curl u| > 0.01."""
+    import oracle
+    v = oracle_mod.voxelize(meshes.box(1.0, 1.0, 1.0, 4), _scaled(0.4), 1.5, 36, 18, 18)
+    s = oracle_mod.Solver(v, u_inlet=0.085, nu=0.005, cs=0.12)
+    s.step(80, threads=oracle_mod.max_threads())
+    m = s.macro()
+    r = oracle.q_criterion(v.nx, v.ny, v.nz, v.dx, m["ux"], m["uy"], m["uz"], v.flags)
+    assert r["maxQ"] > 1e-4
+    assert r["maxOmega"] > 0.01
+
+
+def test_stagnation_and_wake_pressure(oracle_mod):
+    """phase5.test.ts:120-177: the 'cube' preset scaled by 0.45 on 40x20x20, u = 0.08,
+    nu = 0.004, Cs = 0.12, 90 steps: along the centre line the fluid cell in front of
+    the cube has Cp = (rho - 1) / 3 / (u^2 / 2) in (0.65, 1.35), the one behind it Cp < 0."""
+    v = oracle_mod.voxelize(meshes.box(1.0, 1.0, 1.0, 4), _scaled(0.45), 1.5, 40, 20, 20)
+    u = 0.08
+    s = oracle_mod.Solver(v, u_inlet=u, nu=0.004, cs=0.12)
+    s.step(90, threads=oracle_mod.max_threads())
+    nx, ny, nz = v.nx, v.ny, v.nz
+    mid_y, mid_z = ny // 2, nz // 2
+    row = [int(v.flags[ix + nx * (mid_y + ny * mid_z)]) for ix in range(nx)]
+    solid = [ix for ix in range(nx) if row[ix] == 1]
+    windward, leeward = solid[0] - 1, solid[-1] + 1
+    assert 0 < windward < leeward
+    rho = s.macro()["rho"]
+    q_lat = 0.5 * 1.0 * u * u
+    cp = lambda ix: ((1.0 / 3.0) * (float(rho[ix + nx * (mid_y + ny * mid_z)]) - 1.0)) / q_lat
+    assert 0.65 < cp(windward) < 1.35
+    assert cp(leeward) < 0.0
