@@ -12,6 +12,7 @@ answers the reference's test suite asserts:
   phase4.test.ts:119-159  Cd bands of the calibration bodies (testRunner.ts:39-155)
   phase5.test.ts:86-116   vortex cores (Q > 0) in the wake of a cube
   phase5.test.ts:120-177  stagnation Cp near +1 in front of a cube, suction in its wake
+  physicsSuite.test.ts:17-109  monotonic sphere grid convergence about the Morrison Cd
 The meshes are this project's generators standing in for the three.js presets.
 """
 import math
@@ -291,3 +292,39 @@ def test_stagnation_and_wake_pressure(oracle_mod):
     cp = lambda ix: ((1.0 / 3.0) * (float(rho[ix + nx * (mid_y + ny * mid_z)]) - 1.0)) / q_lat
     assert 0.65 < cp(windward) < 1.35
     assert cp(leeward) < 0.0
+
+
+@pytest.mark.slow
+def test_sphere_grid_convergence(oracle_mod):
+    """physicsSuite.test.ts:17-109 (R2.3): the 'sphere' preset in a 6 x 3.6 x 3.6 m tunnel
+    at Re = 400 on 48x24x24 (300 steps), 60x36x36 (350) and 72x48x48 (400); sine^2 ramp
+    over 80 steps to u = 0.08 from 0.001, Cs = 0.12, Maskell-corrected Cd into a 40-sample
+    tracker from 60 % of the run.  The mean Cd falls monotonically with resolution, the
+    coarsest is at or above the Morrison correlation and the finest within 15 % above it."""
+    from aerosim_b200.forces import AIR_20C, ForceConvergenceTracker
+    mesh = meshes.uv_sphere(0.5, 96, 64)
+    a_ref = oracle_mod.frontal_area(mesh)
+    pos = mesh[0]
+    l_ref = float(pos[:, 0].max() - pos[:, 0].min())
+    u, re = 0.08, 400
+    target = _sphere_cd_target(re)
+    t = oracle_mod.max_threads()
+    cds = []
+    for nx, ny, nz, steps in ((48, 24, 24, 300), (60, 36, 36, 350), (72, 48, 48, 400)):
+        v = oracle_mod.voxelize(mesh, None, 3.6, nx, ny, nz)
+        nu = (u * (l_ref / v.dx)) / re
+        s = oracle_mod.Solver(v, u_inlet=0.001, nu=nu, cs=0.12)
+        tr = ForceConvergenceTracker()
+        tr.reset(40)
+        out = None
+        for step in range(1, steps + 1):
+            s.set_params(u_inlet=u * math.sin(0.5 * math.pi * step / 80) ** 2 if step <= 80 else u)
+            s.step(1, threads=t)
+            if step > math.floor(steps * 0.6):
+                me = oracle_mod.momentum_exchange(v, s.f(0))
+                co = oracle_mod.force_coefficients(me["fx"], me["fy"], me["mz"], v.dx, u, a_ref, l_ref, 3.6, 3.6)
+                out = tr.push_sample(s.step_index, co["cd"], co["cl"], co["cm"], co["xcp"], 25.0, AIR_20C, a_ref)
+        cds.append(out["meanCd"])
+    assert cds[0] > cds[1] > cds[2], cds
+    assert cds[0] >= target, (cds, target)
+    assert cds[2] <= target * 1.15, (cds, target)
