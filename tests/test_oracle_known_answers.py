@@ -10,6 +10,7 @@ answers the reference's test suite asserts:
   phase3.test.ts:8-43     Re = 1e5 mass conservation, 10 000 steps
   phase3.test.ts:45-124   Karman street Strouhal number
   phase4.test.ts:119-159  Cd bands of the calibration bodies (testRunner.ts:39-155)
+  physicsSuite.test.ts:111-130  the cube and cylinder bands in developed wakes
   phase5.test.ts:86-116   vortex cores (Q > 0) in the wake of a cube
   phase5.test.ts:120-177  stagnation Cp near +1 in front of a cube, suction in its wake
   physicsSuite.test.ts:17-109  monotonic sphere grid convergence about the Morrison Cd
@@ -188,10 +189,12 @@ BANDS = {  # testRunner.ts / analyticalCases.ts:21-134
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("name", sorted(BANDS))
-def test_cd_band(oracle_mod, name):
+@pytest.mark.parametrize("name,steps", [(n, 350) for n in sorted(BANDS)] + [("cube", 500), ("cylinder", 450)])
+def test_cd_band(oracle_mod, name, steps):
     """runSinglePhysicsBenchmark (testRunner.ts:39-155): 60x36x36, sine^2 ramp over 80
-    steps to u = 0.08, nu = 0.002, Cs = 0.12, 350 steps, mean Cd over a 40-sample window."""
+    steps to u = 0.08, nu = 0.002, Cs = 0.12, mean Cd over a 40-sample window of the
+    second half: 350 steps (phase4.test.ts:119-159), and the developed wakes of the cube
+    (500 steps) and the cylinder (450 steps, physicsSuite.test.ts:111-130)."""
     from aerosim_b200.forces import AIR_20C, ForceConvergenceTracker
     make, band = BANDS[name]
     mesh = make()
@@ -206,10 +209,10 @@ def test_cd_band(oracle_mod, name):
     tr.reset(40)
     out = None
     t = oracle_mod.max_threads()
-    for step in range(1, 351):
+    for step in range(1, steps + 1):
         s.set_params(u_inlet=u * math.sin(0.5 * math.pi * step / 80) ** 2 if step <= 80 else u)
         s.step(1, threads=t)
-        if step > 175:
+        if step > steps // 2:
             me = oracle_mod.momentum_exchange(v, s.f(0))
             co = oracle_mod.force_coefficients(me["fx"], me["fy"], me["mz"], v.dx, u, a_ref, l_ref, 3.6, 3.6)
             out = tr.push_sample(step, co["cd"], co["cl"], co["cm"], co["xcp"], 25.0, AIR_20C, a_ref)
