@@ -89,6 +89,22 @@ def lathe(points: np.ndarray, segments: int, center=(0.0, 0.0, 0.0)) -> Mesh:
     return _finish(pos + np.asarray(center, dtype=np.float64), idx)
 
 
+def ogive_nose(length: float = 1.0, body: float = 0.4, radius: float = 0.25, axial_steps: int = 60,
+               segments: int = 72) -> Mesh:
+    """Tangent-ogive nose cone on a body tube, the shape of the reference's 'rocket_nose'
+    preset (presets.ts:82-111): the profile revolved about y, turned -90 degrees about z
+    so the tip points to -x, and centred on its bounding box."""
+    rho = (radius * radius + length * length) / (2 * radius)
+    pts = [(max(0.0, math.sqrt(max(0.0, rho * rho - (length - x) ** 2)) + radius - rho), x)
+           for x in np.linspace(0, length, axial_steps + 1)]
+    pts += [(radius, length + body), (0.0, length + body)]
+    pos, idx = lathe(np.array(pts), segments)
+    p = pos.astype(np.float64)
+    p = np.stack([p[:, 1], -p[:, 0], p[:, 2]], 1)
+    p -= (p.max(0) + p.min(0)) / 2
+    return p.astype(np.float32), idx
+
+
 def box(sx: float, sy: float, sz: float, segments: int = 4, center=(0.0, 0.0, 0.0)) -> Mesh:
     """Axis-aligned box with each face split into segments x segments quads, wound
     counter-clockwise seen from outside."""

@@ -108,3 +108,25 @@ def test_reference_cube_known_answer_on_gpu(gpu_engine_cls):
     assert r.boundaryCellCount > 2400
     assert r.cellFlags[40 + 80 * (20 + 40 * 20)] == 1
     assert r.cellFlags[2 + 80 * (2 + 40 * 2)] == 0
+
+
+def test_interactive_voxelization_time(gpu_engine_cls, oracle_mod):
+    """phase2.test.ts:130-150: the 'rocket_nose' ogive turned 12 degrees about z in a
+    6 x 2.8 x 2.4 m tunnel on 128x64x64.  After a warm-up call, voxelization with the link
+    q-distances (here the GPU voxelizer and the copy of the whole grid to the host) takes
+    < 50 ms and gives > 100 solid and > 100 boundary cells; the grid is the oracle's."""
+    import time
+    from aerosim_b200 import voxelize_mesh_to_lattice
+    mesh = meshes.ogive_nose()
+    a = math.radians(12.0)
+    world = [math.cos(a), math.sin(a), 0, 0, -math.sin(a), math.cos(a), 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]
+    tunnel = {"length": 6.0, "width": 2.8, "height": 2.4}
+    grid = {"nx": 128, "ny": 64, "nz": 64}
+    voxelize_mesh_to_lattice(mesh, world, tunnel, grid)
+    t0 = time.perf_counter()
+    gpu = voxelize_mesh_to_lattice(mesh, world, tunnel, grid)
+    ms = (time.perf_counter() - t0) * 1e3
+    assert gpu.solidCellCount > 100 and gpu.boundaryCellCount > 100
+    assert gpu.cellFlags[gpu.boundaryCellIndices[0]] == 2
+    assert ms < 50.0, ms
+    _compare(gpu, oracle_mod.voxelize(mesh, world, 2.4, 128, 64, 64))

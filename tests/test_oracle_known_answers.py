@@ -165,26 +165,13 @@ def _sphere_cd_target(re):
     return (24.0 / re) * (1.0 + 0.15 * re ** 0.687) + 0.42 / (1.0 + 42500.0 * re ** -1.16)
 
 
-def _ogive():
-    L, body, R = 1.0, 0.4, 0.25
-    rho = (R * R + L * L) / (2 * R)
-    pts = [(max(0.0, math.sqrt(max(0.0, rho * rho - (L - x) ** 2)) + R - rho), x)
-           for x in np.linspace(0, L, 61)]
-    pts += [(R, L + body), (0.0, L + body)]
-    pos, idx = meshes.lathe(np.array(pts), 72)
-    p = pos.astype(np.float64)
-    p = np.stack([p[:, 1], -p[:, 0], p[:, 2]], 1)  # rotate -90 deg about z: tip at -x
-    p -= (p.max(0) + p.min(0)) / 2
-    return p.astype(np.float32), idx
-
-
 BANDS = {  # testRunner.ts / analyticalCases.ts:21-134
     "cube": (lambda: meshes.box(1.0, 1.0, 1.0, 4), lambda re: (0.88, 1.22)),
     "sphere": (lambda: meshes.uv_sphere(0.5, 96, 64),
                lambda re: (round(_sphere_cd_target(re), 3) * 0.78, round(_sphere_cd_target(re), 3) * 1.25)),
     "cylinder": (lambda: meshes.cylinder(0.3, 1.2, 80, 4),
                  lambda re: ((0.68 + 5.5 / math.sqrt(re)) * 0.8, (0.68 + 5.5 / math.sqrt(re)) * 1.2)),
-    "rocket_nose": (_ogive, lambda re: ((0.2 + 26 / math.sqrt(re)) * 0.8, (0.2 + 26 / math.sqrt(re)) * 1.25)),
+    "rocket_nose": (meshes.ogive_nose, lambda re: ((0.2 + 26 / math.sqrt(re)) * 0.8, (0.2 + 26 / math.sqrt(re)) * 1.25)),
 }
 
 
