@@ -686,7 +686,13 @@ int enqueue_forces(aerosim_engine* h, double* dst, double* dst_dev = nullptr, in
 int ensure_frame_host(aerosim_engine* h) {
   if (h->frame_host) return AEROSIM_OK;
   CU(h, cudaHostAlloc((void**)&h->frame_host, 16 * sizeof(double), cudaHostAllocMapped));
-  CU(h, cudaHostGetDevicePointer((void**)&h->frame_dev, h->frame_host, 0));
+  const cudaError_t e = cudaHostGetDevicePointer((void**)&h->frame_dev, h->frame_host, 0);
+  if (e != cudaSuccess) {  // never keep a host buffer without its device address
+    cudaFreeHost(h->frame_host);
+    h->frame_host = nullptr;
+    h->frame_dev = nullptr;
+    return fail(h, AEROSIM_ERR_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
+  }
   return AEROSIM_OK;
 }
 
