@@ -120,6 +120,8 @@ SIGNATURES = {
                                     _F32P, _F32P, _F32P, _F64P, _F64P], C.c_int),
     "aerosim_mass_stats": ([_P, C.POINTER(Mass)], C.c_int),
     "aerosim_last_step_timing": ([_P, _F64P, C.POINTER(C.c_int64)], C.c_int),
+    "aerosim_step_param_bytes": ([], C.c_int),
+    "aerosim_set_pipeline_wait_limit": ([_P, C.c_int32], C.c_int),
     "aerosim_batch_create": ([C.POINTER(_P), C.c_int32, C.POINTER(_P)], C.c_int),
     "aerosim_batch_destroy": ([_P], C.c_int),
     "aerosim_batch_step": ([_P, C.c_int32], C.c_int),
@@ -128,6 +130,7 @@ SIGNATURES = {
     "aerosim_batch_get_tuning": ([_P, C.POINTER(BatchTuning)], C.c_int),
     "aerosim_batch_last_timing": ([_P, _F64P, C.POINTER(C.c_int64)], C.c_int),
     "aerosim_batch_cells": ([_P, C.POINTER(C.c_int64)], C.c_int),
+    "aerosim_batch_set_pipeline_wait_limit": ([_P, C.c_int32], C.c_int),
     "aerosim_mlp_param_count": ([], C.c_int),
     "aerosim_mlp_forward": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
     "aerosim_mlp_forward_tc": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),

@@ -70,6 +70,7 @@ struct aerosim_engine {
   uint32_t* mlp_frag = nullptr;
   float* mlp_bias = nullptr;
   bool wall_ready = false;  // wall distances in the class bytes
+  int wait_limit = kWaitLimit;  // polls of a step kernel's ring wait before it gives up
 };
 
 namespace {
@@ -636,6 +637,7 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.mlp_bias = h->mlp_bias;
   a.mlp_nu0 = (float)((std::max(a.tau0, 0.5015) - 0.5) / 3.0);
   a.item_groups = h->item_groups;
+  a.wait_limit = h->wait_limit;
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < n; ++s) {
@@ -820,6 +822,14 @@ int aerosim_mass_stats(aerosim_engine* h, aerosim_mass* out) {
   out->rescale_count = s.rescale_count;
   return AEROSIM_OK;
 }
+
+int aerosim_set_pipeline_wait_limit(aerosim_engine* h, int32_t polls) {
+  if (!h) return AEROSIM_ERR_ARG;
+  h->wait_limit = polls < 0 ? kWaitLimit : polls;
+  return AEROSIM_OK;
+}
+
+int aerosim_step_param_bytes(void) { return (int)sizeof(StepArgs); }
 
 int aerosim_last_step_timing(aerosim_engine* h, double* ms, int64_t* launches) {
   if (!h) return AEROSIM_ERR_ARG;
@@ -1175,6 +1185,7 @@ struct aerosim_batch {
   int step = 0;
   double last_ms = 0;
   long long last_launches = 0;
+  int wait_limit = kWaitLimit;  // polls of a ring wait before the batched step gives up
 };
 
 namespace {
@@ -1227,6 +1238,7 @@ BatchArgs batch_args(const aerosim_batch* b, int write_macro) {
   a.geo = b->d_geo;
   a.n_items = b->n_items; a.n_near = b->n_near; a.slot_elems = b->slot_elems; a.slot_cls = b->slot_cls;
   a.n_inst = (int)b->eng.size(); a.stages = b->tune.stages; a.write_macro = write_macro;
+  a.wait_limit = b->wait_limit;
   return a;
 }
 
@@ -1520,6 +1532,18 @@ int aerosim_batch_autotune(aerosim_batch* b, int32_t steps_per_trial, aerosim_ba
   rc = batch_reset(b);
   if (rc) return rc;
   if (out) *out = b->tune;
+  return AEROSIM_OK;
+}
+
+int aerosim_batch_set_pipeline_wait_limit(aerosim_batch* b, int32_t polls) {
+  if (!b) return bfail(AEROSIM_ERR_ARG, "batch_set_pipeline_wait_limit: NULL batch");
+  BCU(cudaSetDevice(b->device));
+  BCU(cudaStreamSynchronize(b->stream));
+  b->wait_limit = polls < 0 ? kWaitLimit : polls;
+  if (b->graph) {  // the captured launches carry the old limit
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
   return AEROSIM_OK;
 }
 

@@ -30,6 +30,7 @@ struct BatchArgs {
   long long slot_elems;          // ring slot stride (elements) and class-byte slot stride
   long long slot_cls;
   int n_inst, stages, write_macro;
+  int wait_limit;                // polls of a ring wait before the step gives up (as StepArgs)
 };
 
 __device__ __forceinline__ int find_instance(const long long* begin, int n, long long x) {
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
     uint32_t ph = 0;
     for (int j = 0; j < my_count; ++j) {
       if (j >= S_) {
-        const bool ok = mbar_wait(&empty[s], ph ^ 1u, kWaitLimit);
+        const bool ok = mbar_wait(&empty[s], ph ^ 1u, b.wait_limit);
         if (!__any_sync(0xffffffffu, ok)) {
           failed = true;
           break;
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
     int offset = 0;  // warp that takes segment 0 of the current item
     for (int j = 0; j < my_count; ++j) {
       {
-        const bool ok = mbar_wait(&full[s], ph, kWaitLimit);
+        const bool ok = mbar_wait(&full[s], ph, b.wait_limit);
         if (!__any_sync(0xffffffffu, ok)) {
           failed = true;
           break;

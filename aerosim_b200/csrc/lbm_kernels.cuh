@@ -77,6 +77,8 @@ struct StepArgs {
   const float* mlp_bias;
   float mlp_nu0;
   int item_groups;        // row groups per work item (16-bit storage kernels; 1 elsewhere)
+  int wait_limit;         // polls of a ring wait before the step gives up (kWaitLimit;
+                          //   0 gives up at once: the failure path's test)
 };
 
 struct ForceArgs {
@@ -1026,7 +1028,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     long long r0 = item_row0;  // first row of this CTA's j-th item
     for (int j = 0; j < my_count; ++j, r0 += item_step) {
       if (j >= S_) {  // the slot's previous fill must have been consumed
-        const bool ok = mbar_wait(&empty[s], ph ^ 1u, kWaitLimit);
+        const bool ok = mbar_wait(&empty[s], ph ^ 1u, a.wait_limit);
         if (!__any_sync(0xffffffffu, ok)) {
           failed = true;
           break;
@@ -1061,8 +1063,9 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
       if (++s == S_) { s = 0; ph ^= 1u; }
     }
     if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
-    // No copy may still be in flight when the CTA exits: wait (bounded) for the
-    // last phase issued into every slot; completed phases return at once.
+    // No copy may still be in flight when the CTA exits: wait (bounded, always with the
+    // full limit) for the last phase issued into every slot; completed phases return at
+    // once.
     if (lane == 0) {
       for (int k = 0; k < S_ && k < issued; ++k) {
         const int last = k + ((issued - 1 - k) / S_) * S_;
@@ -1084,7 +1087,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     long long row0 = item_row0 + ry;  // this warp's row of the item's first group
     for (int j = 0; j < my_count; ++j, row0 += item_step) {
       {
-        const bool ok = mbar_wait(&full[s], ph, kWaitLimit);
+        const bool ok = mbar_wait(&full[s], ph, a.wait_limit);
         if (!__any_sync(0xffffffffu, ok)) {
           failed = true;
           break;

@@ -19,7 +19,14 @@
 // Set-up: the first call on each device, with that device current, resolves the
 // array's device address with cudaGetSymbolAddress (in host code the array's name is
 // only a host-side stand-in, not a device address).  That first call should come
-// before any stream capture on the device.
+// before any stream capture on the device.  The address is kept with the ID of the
+// device's current context: a cudaDeviceReset by the host ends that context and
+// unloads the array with it, so the first call in the new context resolves the address
+// again instead of using the old one.
+//
+// Preconditions the kernel does not check: every boundary_cells[b] lies in
+// [0, nx * ny * nz), and q holds 18 values per boundary cell in the same order.
+#include <cuda.h>  // CUcontext / CUresult types; the driver functions are fetched at run time
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -43,15 +50,47 @@ static __device__ __align__(256) unsigned char g_force_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // context ID the address belongs to
 
-// Device address of g_force_scratch on the current device (resolved once per device).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Process-unique ID of the calling thread's current context (CUDA 12.0 cuCtxGetId, taken
+// from the driver through the runtime, so the library does not link libcuda); 0 when it
+// cannot be read, in which case the address is resolved on every call.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
+
+// Device address of g_force_scratch on the current device: resolved at the first call
+// in each context of the device and kept for the calls that follow.
 cudaError_t scratch_address(int device, void** out) {
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[device]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_scratch_addr[device] || ctx == 0 || ctx != g_scratch_ctx[device]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_force_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_addr[device] = p;
+    g_scratch_ctx[device] = ctx;
   }
   *out = g_scratch_addr[device];
   return cudaSuccess;

@@ -287,6 +287,12 @@ class LBMEngine:
         self._h.call("aerosim_last_step_timing", C.byref(ms), C.byref(n))
         return ms.value, n.value
 
+    def set_pipeline_wait_limit(self, polls: int) -> None:
+        """Polls of a step kernel's ring wait before the step gives up and reports
+        AerosimError(ERR_DEVICE) (negative: the default; 0: give up at once, which runs
+        the failure path on purpose).  reset_flow() clears the error."""
+        self._h.call("aerosim_set_pipeline_wait_limit", int(polls))
+
     def extract_slice_rgba(self, axis: str = "z", fraction: float = 0.5, mode: str = "velocity") -> dict:
         """extractSliceRGBA (lbmCpuReference.ts:499-596) of the last step's macro fields:
         {'width', 'height', 'rgba'} with rgba uint8 [height * width * 4]."""
@@ -429,6 +435,11 @@ class LBMBatch:
         n = C.c_int64()
         N.check(self.lib.aerosim_batch_last_timing(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def set_pipeline_wait_limit(self, polls: int) -> None:
+        """As LBMEngine.set_pipeline_wait_limit for the batched step; autotune() resets
+        a batch whose step failed."""
+        N.check(self.lib.aerosim_batch_set_pipeline_wait_limit(self.h, int(polls)))
 
     @property
     def cells(self) -> int:

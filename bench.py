@@ -69,7 +69,8 @@ def _profile_traffic(precision: str):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples every 100 ms while the timed region runs."""
+    """nvidia-smi clock / throttle samples every 20 ms from before the warm-up to the end
+    of the timed region (a short timed region still gets samples)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -84,7 +85,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -161,11 +162,13 @@ def run_ours(args) -> dict:
     out = {}
     # ---- headline: FP32, device-timed ----
     eng, info = _make_engine(case, "f32", dev)
-    eng.step(args.warmup)
-    barrier_sync()
     with ClockSampler(dev) as clk:
+        time.sleep(0.1)  # the sampler's first rows
+        eng.step(args.warmup)
+        barrier_sync()
         ms, launches = _timed_steps(eng, args.steps)
-    barrier_sync()
+        barrier_sync()
+        time.sleep(0.05)
     ms = max_over_ranks(ms)
     mlups = ws * cells * args.steps / (ms * 1e-3) / 1e6
     hbm, hbm_kind = _peaks()
@@ -198,8 +201,13 @@ def run_ours(args) -> dict:
         dt = max_over_ranks(dt)
         import ctypes
         frame_d2h = ctypes.sizeof(N.Forces) + 4 + fr["rgba"].nbytes
+        # per step, the solver parameters (step index, inlet velocity, tau, buffers) travel
+        # host -> device as the step kernel's argument block, where the reference uploads
+        # its 48-byte SolverParams uniform before every substep (lbmEngine.ts:330-354)
+        step_h2d = int(N.load().aerosim_step_param_bytes())
         out["e2e"] = {"value": round(ws * cells * 4 * frames / dt / 1e6, 1), "unit": "MLUPS",
-                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": frame_d2h // 4,
+                      "h2d_bytes_per_step": step_h2d, "d2h_bytes_per_step": frame_d2h // 4,
+                      "h2d": "step kernel argument block (solver parameters of the step) per launch",
                       "frame": "stepAndExtractSlice: aerosim_step_and_extract_slice (4 substeps, FP64 force sums, "
                                "z = nz/2 velocity RGBA slice, one synchronization), results copied to the host",
                       "frames": frames}
@@ -254,71 +262,11 @@ def run_ours(args) -> dict:
         if ws > 1:  # the same 32-wing sweep split round-robin over the ranks (no exchange)
             out["batch_sharded"] = run_batch(args, dev, ws, barrier_sync, max_over_ranks, shard=(rank, ws))
 
-    # ---- Cd / Cl / Cm error of reduced storage vs the FP64 GPU run.  The flow at
-    # Re = 2e4 is unsteady and chaotic: runs that differ only in rounding follow each
-    # other for the first few thousand steps and then decorrelate.  Two figures per
-    # storage mode: the mean |dCd| over steps 500..3000 relative to the FP64 run's mean
-    # |Cd| (while the runs still track each other), and the difference of the Cd means
-    # over the second half with its standard error (batch means of 10 blocks). ----
+    # ---- Cd / Cl / Cm error of reduced storage vs the FP64 GPU run (cd_vs_fp64) ----
     if args.cd_steps > 0:
-        res = {}
-        every = 50
-        for prec in ("f64", "f32", "f16s", "bf16s"):
-            e3, _ = _make_engine(case, prec, dev)
-            cd, cl, cm, st = [], [], [], []
-            done = 0
-            while done < args.cd_steps:
-                e3.step(every)
-                done += every
-                f = e3.read_forces()
-                cd.append(f.cd); cl.append(f.cl); cm.append(f.cm); st.append(done)
-            m = e3.mass_stats()
-            res[prec] = {"cd": np.array(cd), "cl": np.array(cl), "cm": np.array(cm), "step": np.array(st),
-                         "mass_drift": m["meanRho"] - 1.0, "cumulative_rescale": m["cumulativeRescale"],
-                         "nan": m["hasNaN"]}
-            e3.close()
-
-        def late(x, steps):
-            sel = x[steps > args.cd_steps // 2]
-            blocks = np.array_split(sel, 10)
-            bm = np.array([b.mean() for b in blocks])
-            return float(sel.mean()), float(bm.std(ddof=1) / np.sqrt(len(bm))), float(sel.std())
-
-        ref = res["f64"]
-        early = (ref["step"] >= 500) & (ref["step"] <= 3000)
-        ref_late = late(ref["cd"], ref["step"])
-        summary = {"steps": args.cd_steps, "sample_every": every,
-                   "f64": {"cd_mean_late": ref_late[0], "cd_se_late": ref_late[1], "cd_std_late": ref_late[2],
-                           "mass_drift": ref["mass_drift"], "cumulative_rescale": ref["cumulative_rescale"],
-                           "nan": ref["nan"]}}
-        for p in ("f32", "f16s", "bf16s"):
-            r = res[p]
-            lm = late(r["cd"], r["step"])
-            scale = float(np.mean(np.abs(ref["cd"][early])))
-            summary[p] = {
-                "dcd_rel_early": float(np.mean(np.abs(r["cd"][early] - ref["cd"][early])) / scale),
-                "dcl_abs_early": float(np.mean(np.abs(r["cl"][early] - ref["cl"][early]))),
-                "dcm_abs_early": float(np.mean(np.abs(r["cm"][early] - ref["cm"][early]))),
-                "dcd_mean_rel_late": abs(lm[0] - ref_late[0]) / abs(ref_late[0]),
-                "dcd_mean_rel_late_se": float(np.hypot(lm[1], ref_late[1]) / abs(ref_late[0])),
-                "cd_mean_late": lm[0], "mass_drift": r["mass_drift"], "nan": r["nan"]}
-        # a steady flow separates the storage error from the chaos: the 64x32x32 sphere at
-        # Re = 100, Cd averaged over steps 3500..4000 of each storage mode against FP64
-        sph = cases.sphere_64x32x32()
-        steady = {}
-        for prec in ("f64", "f32", "f16s", "bf16s"):
-            e5, _ = _make_engine(sph, prec, dev)
-            e5.step(3500)
-            vals = []
-            for _ in range(10):
-                e5.step(50)
-                vals.append(e5.read_forces().cd)
-            steady[prec] = float(np.mean(vals))
-            e5.close()
-        summary["steady_sphere_re100"] = {
-            "case": "sphere_64x32x32, u 0.05, Re 100, Cd mean of steps 3500..4000", "cd_f64": steady["f64"],
-            **{f"dcd_rel_{p}": abs(steady[p] - steady["f64"]) / abs(steady["f64"]) for p in ("f32", "f16s", "bf16s")}}
-        out["cd_err_vs_fp64"] = summary
+        out["cd_err_vs_fp64"] = cd_vs_fp64(case, args.cd_steps, dev, blocks=10, steady=True)
+    if args.cd_long_steps > 0:
+        out["cd_err_vs_fp64_long"] = cd_vs_fp64(case, args.cd_long_steps, dev, blocks=20, steady=False)
 
     # ---- CPU baseline: the oracle on one core, bounded sample ----
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -338,6 +286,97 @@ def run_ours(args) -> dict:
                    "parallelism": f"{ws} independent lattices, one per GPU (weak scaling)"},
     })
     return out if rank == 0 else {}
+
+
+def _cd_series(case, prec: str, steps: int, every: int, dev: int, perturb: float = 0.0) -> dict:
+    """Cd / Cl / Cm every `every` steps of one run.  perturb > 0: before the first step,
+    every population's deviation from its rest weight is scaled by (1 + perturb * xi),
+    xi uniform in [-1, 1] from a fixed seed (a rounding-sized perturbation of the start)."""
+    e, _ = _make_engine(case, prec, dev)
+    if perturb > 0.0:
+        f = e.read_populations(np.float64)
+        w = np.repeat(np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12), case.cells)
+        xi = np.random.default_rng(1234).uniform(-1.0, 1.0, f.size)
+        e.write_populations(w + (f - w) * (1.0 + perturb * xi))
+    cd, cl, cm, st = [], [], [], []
+    done = 0
+    while done < steps:
+        e.step(every)
+        done += every
+        f = e.read_forces()
+        cd.append(f.cd); cl.append(f.cl); cm.append(f.cm); st.append(done)
+    m = e.mass_stats()
+    e.close()
+    return {"cd": np.array(cd), "cl": np.array(cl), "cm": np.array(cm), "step": np.array(st),
+            "mass_drift": m["meanRho"] - 1.0, "cumulative_rescale": m["cumulativeRescale"], "nan": m["hasNaN"]}
+
+
+def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True) -> dict:
+    """Cd / Cl / Cm of every storage mode against the FP64 GPU run (FP64 populations and
+    arithmetic).  The flow at Re = 2e4 is unsteady and chaotic: runs that differ only in
+    rounding follow each other for the first few thousand steps and then decorrelate.
+    Per storage mode: the mean |dCd| over steps 500..3000 relative to the FP64 run's mean
+    |Cd| (while the runs still track each other), and the difference of the Cd means over
+    the second half with its standard error (batch means of `blocks` blocks).
+
+    The control `f64_perturbed` is a second FP64 run whose initial populations carry a
+    relative perturbation of FP16's rounding size (2^-11 of each deviation from the rest
+    weight): if it leaves the FP64 run as fast as the FP16 storage does, the early-window
+    difference is the chaos of the flow, not a bias of the storage.  With steady=True the
+    steady 64x32x32 sphere at Re = 100 (Cd averaged over steps 3500..4000) separates the
+    storage error from the chaos."""
+    every = 50
+    res = {p: _cd_series(case, p, steps, every, dev) for p in ("f64", "f32", "f16s", "bf16s")}
+    res["f64_perturbed"] = _cd_series(case, "f64", steps, every, dev, perturb=2.0 ** -11)
+
+    def late(x, st):
+        sel = x[st > steps // 2]
+        bm = np.array([b.mean() for b in np.array_split(sel, blocks)])
+        return float(sel.mean()), float(bm.std(ddof=1) / np.sqrt(len(bm))), float(sel.std())
+
+    ref = res["f64"]
+    early = (ref["step"] >= 500) & (ref["step"] <= 3000)
+    ref_late = late(ref["cd"], ref["step"])
+    summary = {"steps": steps, "sample_every": every, "late_window": f"steps {steps // 2}..{steps}, "
+               f"standard error from {blocks} block means",
+               "f64": {"cd_mean_late": ref_late[0], "cd_se_late": ref_late[1], "cd_std_late": ref_late[2],
+                       "cd_se_late_rel": ref_late[1] / abs(ref_late[0]),
+                       "mass_drift": ref["mass_drift"], "cumulative_rescale": ref["cumulative_rescale"],
+                       "nan": ref["nan"]}}
+    scale = float(np.mean(np.abs(ref["cd"][early]))) if early.any() else float("nan")
+    for p in ("f32", "f16s", "bf16s", "f64_perturbed"):
+        r = res[p]
+        lm = late(r["cd"], r["step"])
+        d = {"dcd_mean_rel_late": abs(lm[0] - ref_late[0]) / abs(ref_late[0]),
+             "dcd_mean_rel_late_se": float(np.hypot(lm[1], ref_late[1]) / abs(ref_late[0])),
+             "cd_mean_late": lm[0], "mass_drift": r["mass_drift"], "nan": r["nan"]}
+        if early.any():
+            d.update({"dcd_rel_early": float(np.mean(np.abs(r["cd"][early] - ref["cd"][early])) / scale),
+                      "dcl_abs_early": float(np.mean(np.abs(r["cl"][early] - ref["cl"][early]))),
+                      "dcm_abs_early": float(np.mean(np.abs(r["cm"][early] - ref["cm"][early])))})
+            # first sample where the run leaves the FP64 run by more than 1 % of mean |Cd|
+            dev_idx = np.nonzero(np.abs(r["cd"] - ref["cd"]) > 0.01 * scale)[0]
+            d["first_step_dcd_gt_1pct"] = int(r["step"][dev_idx[0]]) if dev_idx.size else None
+        summary[p] = d
+    summary["f64_perturbed"]["perturbation"] = "initial deviations from the rest weights x (1 + 2^-11 xi), " \
+                                               "xi uniform in [-1, 1]"
+    if steady:
+        from aerosim_b200 import cases
+        sph = cases.sphere_64x32x32()
+        vals = {}
+        for prec in ("f64", "f32", "f16s", "bf16s"):
+            e5, _ = _make_engine(sph, prec, dev)
+            e5.step(3500)
+            cds = []
+            for _ in range(10):
+                e5.step(50)
+                cds.append(e5.read_forces().cd)
+            vals[prec] = float(np.mean(cds))
+            e5.close()
+        summary["steady_sphere_re100"] = {
+            "case": "sphere_64x32x32, u 0.05, Re 100, Cd mean of steps 3500..4000", "cd_f64": vals["f64"],
+            **{f"dcd_rel_{p}": abs(vals[p] - vals["f64"]) / abs(vals["f64"]) for p in ("f32", "f16s", "bf16s")}}
+    return summary
 
 
 def closure_forward_tiles(params, rows: int, reps: int = 3) -> dict:
@@ -481,6 +520,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cd-steps", type=int, default=20000, help="steps of the FP64-oracle Cd comparison (0: skip)")
+    ap.add_argument("--cd-long-steps", type=int, default=0,
+                    help="steps of a second, long FP64-oracle Cd comparison for late-window means (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--sgs-steps", type=int, default=2000,
                     help="steps of the 256x128x128 case with the learned closure (0: skip)")

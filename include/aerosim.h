@@ -183,6 +183,23 @@ int aerosim_step_and_extract_slice(aerosim_engine* h, int32_t n, int32_t axis, d
  * engine's stream) and the number of kernels it launched. */
 int aerosim_last_step_timing(aerosim_engine* h, double* ms, int64_t* kernel_launches);
 
+/* Bytes of solver parameters that travel host -> device with every step launch (the
+ * kernel's argument block: step index, inlet velocity, tau, buffers).  The reference
+ * uploads its SolverParams uniform (48 B) before every substep, lbmEngine.ts:330-354,484. */
+int aerosim_step_param_bytes(void);
+
+/* ---- failure path of the step kernels ----------------------------------------- */
+
+/* Every ring wait of the step kernel (a consumer warp waiting for a bulk copy, the
+ * producer waiting for a free slot) gives up after `polls` polls, sets the engine's
+ * device error flag and lets the CTA return (after waiting, with the full limit, for
+ * its own copies still in flight); the step call then returns AEROSIM_ERR_DEVICE and
+ * aerosim_reset_flow clears the flag.  polls < 0 restores the default (2^22); 0 gives up
+ * without polling, which makes the failure path run on purpose (tests).  The
+ * reference's counterpart is the isBusy / null result of stepAndExtractSlice,
+ * lbmEngine.ts:420, 593-600: a step that cannot complete reports it instead of hanging. */
+int aerosim_set_pipeline_wait_limit(aerosim_engine* h, int32_t polls);
+
 /* ---- allocation-free force reduction ------------------------------------------ */
 
 /* Momentum-exchange forces (the reduction of aerosim_read_forces) over device buffers
@@ -190,14 +207,17 @@ int aerosim_last_step_timing(aerosim_engine* h, double* ms, int64_t* kernel_laun
  * reference: it serves hosts that own all device memory through their own allocator
  * and may not call cudaMalloc, and frame loops that cannot afford its synchronisation.
  * f: device float[19 * N], dense f[d * N + idx]; flags: device u8[N] (0 fluid, 1 solid,
- * 2 boundary); boundary_cells: device i32[B]; q: device f32[B * 18]; out: device
- * double[8] = fx, fy, fz, mx, my, mz (lattice units, moments about the domain centre),
- * cut face links, CTAs used.  stream: a cudaStream_t (NULL: the legacy default stream);
+ * 2 boundary); boundary_cells: device i32[B], each in [0, N) (not checked on the
+ * device: an index outside the lattice reads out of bounds); q: device f32[B * 18],
+ * q[b * 18 + d - 1] for link d of boundary_cells[b]; out: device double[8] = fx, fy, fz,
+ * mx, my, mz (lattice units, moments about the domain centre), cut face links, CTAs
+ * used (ceil(B / 256)).  stream: a cudaStream_t (NULL: the legacy default stream);
  * the work is enqueued, not waited for.  Limit: B <= 1 048 576 (4096 CTAs); larger B
  * returns AEROSIM_ERR_ARG.  Scratch is a fixed per-device array shared by all calls:
  * calls whose kernels overlap on the GPU race.  The first call on a device resolves the
- * array's address and should come before any stream capture on that device.  Errors
- * are reported through aerosim_last_error(NULL). */
+ * array's address and should come before any stream capture on that device; after a
+ * cudaDeviceReset the first call in the new context resolves it again.  Errors are
+ * reported through aerosim_last_error(NULL). */
 int aerosim_momentum_exchange_noalloc(const float* f, const uint8_t* flags, const int32_t* boundary_cells,
                                       const float* q, int64_t boundary_count, int32_t nx, int32_t ny,
                                       int32_t nz, double* out, void* stream);
@@ -292,6 +312,9 @@ int aerosim_batch_step(aerosim_batch* b, int32_t n);
 int aerosim_batch_autotune(aerosim_batch* b, int32_t steps_per_trial, aerosim_batch_tuning* out);
 int aerosim_batch_set_tuning(aerosim_batch* b, const aerosim_batch_tuning* t);
 int aerosim_batch_get_tuning(aerosim_batch* b, aerosim_batch_tuning* out);
+/* The ring-wait limit of the batched step kernel, as aerosim_set_pipeline_wait_limit;
+ * a failed step returns AEROSIM_ERR_DEVICE until the next autotune resets the batch. */
+int aerosim_batch_set_pipeline_wait_limit(aerosim_batch* b, int32_t polls);
 /* Device time (CUDA events) and kernel launches of the last aerosim_batch_step call. */
 int aerosim_batch_last_timing(aerosim_batch* b, double* ms, int64_t* kernel_launches);
 /* Cells of all instances (the MLUPS numerator of one batched step). */

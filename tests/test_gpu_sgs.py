@@ -128,3 +128,39 @@ def test_trained_closure_runs_stably_and_samples_are_sane():
     coarse.step(10)
     for e in eng:
         e.close()
+
+
+def test_trained_closure_beats_smagorinsky_on_held_out_samples():
+    """What the trained network gains over the method without it.  The solver generates
+    a fine 128x64x64 run of the perturbed ellipsoid (Smagorinsky, FP32); its flow,
+    box-filtered onto the 2x coarser 64x32x32 lattice, gives the eddy viscosity the coarse
+    grid needs (least-squares fit of the filtered subgrid stress per cell).  The network
+    is trained on one snapshot and scored on a later one it has not seen: its nu_t / nu_0
+    must have a clearly lower mean squared error than the Smagorinsky eddy viscosity of
+    the same cells (lbmCpuReference.ts:264-282, the closure it replaces), and lower than
+    predicting no eddy viscosity at all."""
+    fine_case = cases.scaled_ellipsoid(128, 64, 64)
+    coarse_case = cases.scaled_ellipsoid(64, 32, 32)
+    eng = []
+    for c in (fine_case, coarse_case):
+        e = LBMEngine(0)
+        e.voxelize(c.mesh, None, c.tunnel, {"nx": c.nx, "ny": c.ny, "nz": c.nz},
+                   {"uInletLattice": c.u_inlet, "nuLattice": c.nu, "smagorinskyCs": c.cs, "precision": "f32"})
+        eng.append(e)
+    fine, coarse = eng
+    fine.step(1600)
+    Xt, Yt = sgs.samples(fine, coarse)
+    fine.step(400)
+    Xv, Yv = sgs.samples(fine, coarse)
+    for e in eng:
+        e.close()
+    assert Xt.shape[0] > 20000 and Xv.shape[0] > 20000
+    p, curve = sgs.train(sgs.init_params(0), Xt, Yt, iters=1500, batch=8192, lr=2e-3, seed=0)
+    assert np.all(np.isfinite(curve))
+    nu0 = (max(3.0 * coarse_case.nu + 0.5, 0.5015) - 0.5) / 3.0
+    mse_mlp = float(np.mean((sgs.forward(p, Xv).astype(np.float64) - Yv) ** 2))
+    mse_smag = float(np.mean((sgs.smagorinsky_ratio(Xv, nu0, coarse_case.cs) - Yv) ** 2))
+    mse_zero = float(np.mean(Yv.astype(np.float64) ** 2))
+    print(f"held-out MSE of nu_t/nu_0: closure {mse_mlp:.4g}, Smagorinsky {mse_smag:.4g}, zero {mse_zero:.4g}")
+    assert mse_mlp < 0.9 * mse_smag, (mse_mlp, mse_smag)
+    assert mse_mlp < mse_zero, (mse_mlp, mse_zero)
