@@ -29,6 +29,9 @@ BYTES_PER_CELL = {PREC_F32: 152, PREC_F32_MIRROR: 152, PREC_F16S: 76, PREC_BF16S
 
 DTYPE_F32, DTYPE_F64 = 0, 1
 
+SGS_PATH_DEFAULT, SGS_PATH_WARP, SGS_PATH_TCGEN05 = 0, 1, 2
+SGS_PATHS = {"default": SGS_PATH_DEFAULT, "mma_sync": SGS_PATH_WARP, "tcgen05": SGS_PATH_TCGEN05}
+
 
 class AerosimError(RuntimeError):
     def __init__(self, code: int, msg: str):
@@ -140,6 +143,7 @@ SIGNATURES = {
     "aerosim_mlp_train": ([_F32P, _F32P, _F32P, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _F32P],
                           C.c_int),
     "aerosim_set_sgs_mlp": ([_P, _F32P], C.c_int),
+    "aerosim_set_sgs_mlp_path": ([_P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "aerosim_read_wall_distance": ([_P, _F32P], C.c_int),
     "aerosim_sgs_samples": ([_P, _P, C.c_float, C.c_int32, _F32P, _F32P, _U8P], C.c_int),
     "aerosim_frontal_area": ([_F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P], C.c_int),

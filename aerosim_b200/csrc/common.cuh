@@ -204,6 +204,7 @@ __host__ inline Layout make_reference_layout(int nx, int ny, int nz) {
 struct StepState {
   unsigned long long rho_sum[2];   // fixed-point sum of post-boundary densities
   unsigned int ticket[2];          // CTA completion counters (last-CTA finalisation)
+  unsigned int next_item[2];       // next work item of step s handed to a CTA (dynamic deal)
   int apply[2];                    // 1 if step s triggered the mean-density rescale
   double corr[2];                  // 1 / meanRho of step s
   double cumulative_rescale;       // product of applied corrections

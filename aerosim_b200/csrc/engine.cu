@@ -40,11 +40,14 @@ struct aerosim_engine {
   size_t smem = 0;
   int stages = 3;
   int item_groups = 1;  // row groups per work item of the step kernel
+  int cells_per_thread = 1;  // consumer cells per thread of the step kernel (1 or 2)
+  int dynamic_items = 0;     // work items from a device counter (1) or dealt round-robin (0)
   int occupancy = 0;
   int num_sms = 148;
   float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
   int32_t* near_cells = nullptr;  // near-wall cells and their link table
   NearLink* links = nullptr;
+  NearLinkF* links_f = nullptr;  // compact table of the FP32-arithmetic kernels
   long long n_near = 0;
   double* abl = nullptr;
   double* sin_tab = nullptr;
@@ -69,6 +72,8 @@ struct aerosim_engine {
   // learned SGS closure (null: Smagorinsky)
   uint32_t* mlp_frag = nullptr;
   float* mlp_bias = nullptr;
+  uint4* mlp_umma = nullptr;  // weight image of the tcgen05 path
+  int mlp_path = AEROSIM_SGS_PATH_DEFAULT;
   bool wall_ready = false;  // wall distances in the class bytes
   int wait_limit = kWaitLimit;  // polls of a step kernel's ring wait before it gives up
 };
@@ -134,6 +139,15 @@ int do_reset(aerosim_engine* h) {
   return AEROSIM_OK;
 }
 
+// The tcgen05 weight image when the closure runs as 128-cell tcgen05 tiles: that path was
+// chosen and the lattice's row pitch is 128 or 256 (every work item then keeps the 8
+// consumer warps busy as two groups of four); otherwise null (warp-level mma.sync).
+const uint4* closure_umma(const aerosim_engine* h) {
+  if (!h->mlp_frag || !h->mlp_umma || !h->have_grid) return nullptr;
+  const bool fits = h->L.pitch == 128 || h->L.pitch == 256;
+  return (h->mlp_path == AEROSIM_SGS_PATH_TCGEN05 && fits) ? h->mlp_umma : nullptr;
+}
+
 // Chooses the persistent step-kernel launch: CTAs of 8 consumer warps + 1 producer
 // warp, as many resident per SM as registers and shared memory allow, and the
 // deepest shared-memory ring (up to 4 slots) that keeps that residency.
@@ -144,15 +158,29 @@ int configure_step(aerosim_engine* h) {
   StepArgs dummy{};
   dummy.L = L;  // the kernel instance depends on the row pitch and the closure
   dummy.mlp_frag = h->mlp_frag;
-  const bool mlp = h->mlp_frag != nullptr;
-  const bool grouped = !mlp && (h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S);
-  const int groups = grouped ? item_groups_for(L.nx) : 1;
+  dummy.mlp_umma = closure_umma(h);
+  const int mlp = h->mlp_frag ? (dummy.mlp_umma ? 2 : 1) : 0;
+  const bool half = h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S;
+  const bool fast = half || h->cfg.precision == AEROSIM_PREC_F32;
+  // two cells per consumer thread (packed FP32 pairs) for the 16-bit storage kernels
+  // without the closure on rows of an even cell count; AEROSIM_CELLS_PER_THREAD (1 or 2)
+  // overrides the choice for any fast-mode lattice that allows it
+  const bool pairs_fit = !mlp && L.nx % 2 == 0 && L.nx >= 4;
+  int cpt = (half && pairs_fit) ? 2 : 1;
+  if (const char* cenv = getenv("AEROSIM_CELLS_PER_THREAD")) {
+    const int want = atoi(cenv);
+    if (want == 1) cpt = 1;
+    if (want == 2 && fast && pairs_fit) cpt = 2;
+  }
+  dummy.cells_per_thread = cpt;
+  const bool grouped = !mlp && half;
+  const int groups = grouped ? item_groups_for(L.nx, cpt) : 1;
   const char* env = getenv("AEROSIM_STAGES");
   const int forced = env ? atoi(env) : 0;
   int best_s = 0, best_occ = 0;
   for (int S = 2; S <= 8; ++S) {
     if (forced && S != forced) continue;
-    const size_t smem = step_smem_bytes(L, S, eb, mlp, groups);
+    const size_t smem = step_smem_bytes(L, S, eb, mlp, groups, cpt);
     if (smem > 227 * 1024) break;
     int occ = 0;
     cudaError_t e = launch_step(h->cfg.precision, dummy, block, 0, smem, h->stream, &occ, nullptr);
@@ -166,12 +194,15 @@ int configure_step(aerosim_engine* h) {
   if (best_s == 0) return fail(h, AEROSIM_ERR_ARG, "step kernel: no launch configuration fits shared memory");
   h->block = block;
   h->stages = best_s;
-  h->smem = step_smem_bytes(L, best_s, eb, mlp, groups);
+  h->smem = step_smem_bytes(L, best_s, eb, mlp, groups, cpt);
   h->item_groups = groups;
+  h->cells_per_thread = cpt;
+  // AEROSIM_DYNAMIC_ITEMS (0 or 1) overrides the deal of the work items
+  if (const char* denv = getenv("AEROSIM_DYNAMIC_ITEMS")) h->dynamic_items = atoi(denv) ? 1 : 0;
   // the occupancy of the chosen configuration
   CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ, nullptr));
   h->occupancy = best_occ;
-  const long long item_rows = (long long)rows_per_item(L.nx) * groups;
+  const long long item_rows = (long long)rows_per_item(L.nx, cpt) * groups;
   const long long items = ((long long)L.ny * L.nz + item_rows - 1) / item_rows;
   long long grid = (long long)best_occ * h->num_sms;
   const char* genv = getenv("AEROSIM_CTAS_PER_SM");
@@ -315,13 +346,18 @@ int install_grid(aerosim_engine* h, DevGrid& ng, double dx, const double origin[
         }
       }
     }
-    cudaFree(h->near_cells); cudaFree(h->links);
-    h->near_cells = nullptr; h->links = nullptr;
+    std::vector<NearLinkF> links_f(links.size());
+    for (size_t i = 0; i < links.size(); ++i)
+      links_f[i] = NearLinkF{links[i].o1, links[i].o2, (float)links[i].A, (float)links[i].B};
+    cudaFree(h->near_cells); cudaFree(h->links); cudaFree(h->links_f);
+    h->near_cells = nullptr; h->links = nullptr; h->links_f = nullptr;
     h->n_near = nn;
     CU(h, cudaMalloc(&h->near_cells, std::max<long long>(nn, 1) * 4));
     CU(h, cudaMalloc(&h->links, links.size() * sizeof(NearLink)));
+    CU(h, cudaMalloc(&h->links_f, links_f.size() * sizeof(NearLinkF)));
     if (nn) CU(h, cudaMemcpy(h->near_cells, nearv.data(), nn * 4, cudaMemcpyHostToDevice));
     CU(h, cudaMemcpy(h->links, links.data(), links.size() * sizeof(NearLink), cudaMemcpyHostToDevice));
+    CU(h, cudaMemcpy(h->links_f, links_f.data(), links_f.size() * sizeof(NearLinkF), cudaMemcpyHostToDevice));
   }
   h->wall_ready = false;
   if (h->mlp_frag) {  // the learned closure reads wall distances from the class bytes
@@ -439,12 +475,12 @@ int aerosim_destroy(aerosim_engine* h) {
   free_grid(h->g);
   free_pops(h);
   cudaFree(h->abl); cudaFree(h->sin_tab); cudaFree(h->st);
-  cudaFree(h->near_cells); cudaFree(h->links);
+  cudaFree(h->near_cells); cudaFree(h->links); cudaFree(h->links_f);
   cudaFree(h->force_partials); cudaFree(h->force_ticket); cudaFree(h->force_out);
   cudaFree(h->stats_buf); cudaFree(h->staging);
   if (h->frame_host) cudaFreeHost(h->frame_host);
   if (h->slice_host) cudaFreeHost(h->slice_host);
-  cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
+  cudaFree(h->mlp_frag); cudaFree(h->mlp_bias); cudaFree(h->mlp_umma);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -627,6 +663,7 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.L = h->L; a.fluid_count = h->fluid_count;
   a.near_cells = h->near_cells; a.n_near = h->n_near;
   a.links = h->links;
+  a.links_f = h->links_f;
   a.stages = h->stages;
   a.ground_no_slip = h->cfg.ground_no_slip;
   a.u_inlet = h->cfg.u_inlet_lattice;
@@ -635,8 +672,11 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.k_smag = 18.0 * M_SQRT2 * cs2;
   a.mlp_frag = h->mlp_frag;
   a.mlp_bias = h->mlp_bias;
+  a.mlp_umma = closure_umma(h);
   a.mlp_nu0 = (float)((std::max(a.tau0, 0.5015) - 0.5) / 3.0);
   a.item_groups = h->item_groups;
+  a.cells_per_thread = h->cells_per_thread;
+  a.dynamic_items = h->dynamic_items;
   a.wait_limit = h->wait_limit;
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
@@ -1079,27 +1119,48 @@ int aerosim_set_sgs_mlp(aerosim_engine* h, const float* params) {
   if (!h) return AEROSIM_ERR_ARG;
   CU(h, cudaSetDevice(h->device));
   if (!params) {
-    cudaFree(h->mlp_frag); cudaFree(h->mlp_bias);
+    cudaFree(h->mlp_frag); cudaFree(h->mlp_bias); cudaFree(h->mlp_umma);
     h->mlp_frag = nullptr;
     h->mlp_bias = nullptr;
+    h->mlp_umma = nullptr;
   } else {
     for (int i = 0; i < kMlpParams; ++i)
       if (!std::isfinite(params[i])) return fail(h, AEROSIM_ERR_ARG, "set_sgs_mlp: non-finite parameter");
     std::vector<uint32_t> frag(kMlpFragWords * 32);
     std::vector<float> bias(kMlpBias);
     mlp_pack_fragments(params, frag.data(), bias.data());
+    std::vector<uint16_t> img(kUmmaBBytes / 2);
+    mlp_pack_umma(params, img.data());
     if (!h->mlp_frag) {
       CU(h, cudaMalloc(&h->mlp_frag, frag.size() * sizeof(uint32_t)));
       CU(h, cudaMalloc(&h->mlp_bias, bias.size() * sizeof(float)));
+      CU(h, cudaMalloc(&h->mlp_umma, kUmmaBBytes));
     }
     CU(h, cudaMemcpy(h->mlp_frag, frag.data(), frag.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     CU(h, cudaMemcpy(h->mlp_bias, bias.data(), bias.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CU(h, cudaMemcpy(h->mlp_umma, img.data(), kUmmaBBytes, cudaMemcpyHostToDevice));
     if (h->have_grid) {
       int rc = ensure_wall_distance(h);
       if (rc) return rc;
     }
   }
   if (h->have_grid && h->f[0]) return configure_step(h);
+  return AEROSIM_OK;
+}
+
+int aerosim_set_sgs_mlp_path(aerosim_engine* h, int32_t path, int32_t* in_use) {
+  if (!h) return AEROSIM_ERR_ARG;
+  if (path != AEROSIM_SGS_PATH_DEFAULT && path != AEROSIM_SGS_PATH_WARP && path != AEROSIM_SGS_PATH_TCGEN05)
+    return fail(h, AEROSIM_ERR_ARG, "set_sgs_mlp_path: unknown path");
+  CU(h, cudaSetDevice(h->device));
+  h->mlp_path = path;
+  if (h->have_grid && h->f[0]) {
+    const int rc = configure_step(h);
+    if (rc) return rc;
+  }
+  if (in_use)
+    *in_use = !h->mlp_frag ? AEROSIM_SGS_PATH_DEFAULT
+                           : (closure_umma(h) ? AEROSIM_SGS_PATH_TCGEN05 : AEROSIM_SGS_PATH_WARP);
   return AEROSIM_OK;
 }
 
@@ -1221,7 +1282,7 @@ int batch_upload_table(aerosim_batch* b) {
     a.mux = e->mux; a.muy = e->muy; a.muz = e->muz; a.mrho = e->mrho;
     a.abl = e->abl; a.sin_tab = e->sin_tab; a.st = e->st;
     a.L = e->L; a.fluid_count = e->fluid_count;
-    a.near_cells = e->near_cells; a.n_near = e->n_near; a.links = e->links;
+    a.near_cells = e->near_cells; a.n_near = e->n_near; a.links = e->links; a.links_f = e->links_f;
     a.ground_no_slip = e->cfg.ground_no_slip;
     a.u_inlet = e->cfg.u_inlet_lattice;
     a.tau0 = 3.0 * e->cfg.nu_lattice + 0.5;

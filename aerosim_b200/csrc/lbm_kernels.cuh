@@ -20,6 +20,8 @@
 #pragma once
 #include "common.cuh"
 #include "sgs_mlp.cuh"
+#include "sgs_umma.cuh"
+#include "lbm_pair.cuh"
 
 namespace aerosim {
 
@@ -30,9 +32,13 @@ enum { MODE_FAST = 0, MODE_MIRROR = 1, MODE_F64 = 2 };
 // 256x128x128, with some spilling at 64 registers); the 16-bit storage kernels issue
 // more instructions per cell and lose more to spills at that budget, so they keep two.
 // With the learned closure the tensor-core MLP needs registers: two CTAs.
-template <class S, int MODE, bool MLP = false>
+// MLP: 0 Smagorinsky, 1 the closure as warp-level mma.sync tiles, 2 the closure as
+// 128-cell tcgen05 tiles (groups of four consumer warps, TMEM accumulators).
+enum { MLP_NONE = 0, MLP_WARP = 1, MLP_TCGEN05 = 2 };
+// Two cells per thread (CPT = 2) hold twice the values: two CTAs for every storage.
+template <class S, int MODE, int MLP = MLP_NONE, int CPT = 1>
 constexpr int step_min_blocks() {
-  return MODE != MODE_FAST ? 1 : (MLP ? 2 : (sizeof(typename S::T) == 4 ? 3 : 2));
+  return MODE != MODE_FAST ? 1 : ((MLP || CPT == 2) ? 2 : (sizeof(typename S::T) == 4 ? 3 : 2));
 }
 // Row groups per work item of the step kernel: a work item holds item_groups x
 // rows_per_item(nx) x-rows and every consumer warp takes its segment of each group, so
@@ -41,12 +47,13 @@ constexpr int step_min_blocks() {
 // per step at 256x128x128; the group count is StepArgs::item_groups); FP32 keeps one
 // group, because its larger ring slots would cost a resident CTA per SM (118.6 -> 127.6
 // us with 2 groups).
-template <class S, int MODE, bool MLP = false>
+template <class S, int MODE, int MLP = MLP_NONE>
 constexpr bool step_item_grouped() {
   return MODE == MODE_FAST && !MLP && sizeof(typename S::T) == 2;
 }
 
 struct NearLink;
+struct NearLinkF;
 
 struct StepArgs {
   const void* fsrc;
@@ -66,6 +73,7 @@ struct StepArgs {
   const int32_t* near_cells;  // cells with a solid pull source, x faces excluded
   long long n_near;
   const NearLink* links;      // [19][n_near] link table of the near-wall cells
+  const NearLinkF* links_f;   // [19][n_near] the same, compact, for the FP32-arithmetic kernels
   int stages;             // depth of the shared-memory ring
   int step_index;
   int write_macro;
@@ -75,10 +83,14 @@ struct StepArgs {
   // (sgs_mlp.cuh) and the molecular viscosity nu_0 its output is scaled by
   const uint32_t* mlp_frag;
   const float* mlp_bias;
+  const uint4* mlp_umma;  // weight image of the tcgen05 path (sgs_umma.cuh), or null
   float mlp_nu0;
   int item_groups;        // row groups per work item (16-bit storage kernels; 1 elsewhere)
   int wait_limit;         // polls of a ring wait before the step gives up (kWaitLimit;
                           //   0 gives up at once: the failure path's test)
+  int cells_per_thread;   // consumer cells per thread: 1, or 2 (pair kernels, even nx)
+  int dynamic_items;      // 1: CTAs take work items from a device counter (StepState::next_item)
+                          //   instead of the static round-robin deal
 };
 
 struct ForceArgs {
@@ -318,9 +330,10 @@ struct MlpRefs {
   float nu0;
   float wall_dist;       // this lane's cell
   int lane;
+  UmmaGroup* grp;        // the tcgen05 path: this warp's group state
 };
 
-template <class S, bool MLP = false>
+template <class S, int MLP = MLP_NONE>
 __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux, float& uy, float& uz,
                                              float tau0, float k_smag, float2 dec, const MlpRefs* m = nullptr) {
   static_assert(S::kRawMoments, "the FP32 collision runs on stored deviations");
@@ -369,10 +382,12 @@ __device__ __forceinline__ void collide_fast(float (&h)[19], float& r, float& ux
   const float off = fmaf(pxy, pxy, fmaf(pxz, pxz, pyz * pyz));
   const float pn = sqrt_approx(fmaf(pxx, pxx, fmaf(pyy, pyy, fmaf(pzz, pzz, 2.0f * off))));
   float tau = 0.5f * (tau0 + sqrt_approx(fmaf(tau0, tau0, k_smag * pn * ir)));
-  if constexpr (MLP) {
+  if constexpr (MLP != MLP_NONE) {
     float x[kMlpIn];
     mlp_features(pxx, pyy, pzz, pxy, pxz, pyz, r, tau, m->wall_dist, x);
-    const float ratio = mlp_nut_warp(x, m->frag, m->bias, m->stage, m->lane);
+    float ratio;
+    if constexpr (MLP == MLP_TCGEN05) ratio = mlp_nut_umma(x, *m->grp, m->bias);
+    else ratio = mlp_nut_warp(x, m->frag, m->bias, m->stage, m->lane);
     const float tm = fmaf(3.0f * m->nu0, 1.0f + ratio, 0.5f);
     if (tm == tm && tm < 1.0e30f) tau = tm;
   }
@@ -469,19 +484,24 @@ constexpr int kHelperWarp = kConsumerWarps + 1;        // warp 9: near-wall cell
 constexpr int kStepThreads = (kConsumerWarps + 2) * 32;
 enum { STEP_ERR_PIPELINE_TIMEOUT = 1 };
 
-// Thread -> cell mapping of a row: cell ix = slot - shift with slot = lane + 32 * warp
-// + tx_span * chunk.  shift = 1 when nx = 1 (mod 32) keeps the cell pairs (0, 1) and
-// (nx-2, nx-1) inside one warp, so the inlet and outlet exchange stays warp-local.
-__host__ __device__ inline int row_shift(int nx) { return (nx % 32 == 1) ? 1 : 0; }
-__host__ __device__ inline int row_span(int nx) {  // threads along x (multiple of 32, <= 256)
-  const int t = (nx + row_shift(nx) + 31) / 32 * 32;
+// Thread -> cell mapping of a row.  One cell per thread (cpt = 1): cell ix = slot - shift
+// with slot = lane + 32 * warp + tx_span * chunk; shift = 1 when nx = 1 (mod 32) keeps
+// the cell pairs (0, 1) and (nx-2, nx-1) inside one warp, so the inlet and outlet
+// exchange stays warp-local.  Two cells per thread (cpt = 2, rows of an even cell count):
+// thread slot holds cells 2 slot and 2 slot + 1, so each row end sits in one thread with
+// the neighbour its boundary condition reads, and no shift is needed.
+__host__ __device__ inline int row_shift(int nx, int cpt = 1) { return (cpt == 1 && nx % 32 == 1) ? 1 : 0; }
+__host__ __device__ inline int row_span(int nx, int cpt = 1) {  // threads along x (multiple of 32, <= 256)
+  const int t = ((nx + row_shift(nx, cpt) + cpt - 1) / cpt + 31) / 32 * 32;
   return t > kConsumerWarps * 32 ? kConsumerWarps * 32 : t;
 }
-__host__ __device__ inline int rows_per_item(int nx) { return (kConsumerWarps * 32) / row_span(nx); }
+__host__ __device__ inline int rows_per_item(int nx, int cpt = 1) {
+  return (kConsumerWarps * 32) / row_span(nx, cpt);
+}
 // Row groups per work item for about 1024 cells per item (1..4).
-__host__ __device__ inline int item_groups_for(int nx) {
-  const int span = row_span(nx), chunks = (nx + row_shift(nx) + span - 1) / span;
-  const int cells = rows_per_item(nx) * chunks * span;
+__host__ __device__ inline int item_groups_for(int nx, int cpt = 1) {
+  const int span = row_span(nx, cpt) * cpt, chunks = (nx + row_shift(nx, cpt) + span - 1) / span;
+  const int cells = rows_per_item(nx, cpt) * chunks * span;
   return cells >= 1024 ? 1 : (1024 / cells > 4 ? 4 : 1024 / cells);
 }
 
@@ -491,17 +511,20 @@ __host__ __device__ inline int item_groups_for(int nx) {
 // slots' destination rows; a guard; a full and an empty mbarrier per slot; the inlet
 // tables ux_in[ny], uy_in[ny]; the row coordinates [stages][groups x RY]; per consumer warp an outlet scratch row of 20
 // floats; the per-lane direction table (c_x, c_y, c_z, w; slot) of the row-end cells.
-__host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem, int groups = 1) {
-  return (size_t)rows_per_item(L.nx) * groups * (19 * (size_t)L.pitch * elem + (size_t)L.pitch);
+__host__ __device__ inline size_t step_stage_bytes(const Layout& L, size_t elem, int groups = 1, int cpt = 1) {
+  return (size_t)rows_per_item(L.nx, cpt) * groups * (19 * (size_t)L.pitch * elem + (size_t)L.pitch);
 }
 constexpr size_t kSmemGuard = 64;
-// With the learned closure: its weight fragments, biases and per-warp staging blocks.
-__host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem, bool mlp = false,
-                                                   int groups = 1) {
-  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem, groups) + kSmemGuard + 16 + 16 * (size_t)stages +
-         2 * (size_t)L.ny * sizeof(double) + (size_t)stages * rows_per_item(L.nx) * groups * sizeof(int2) +
-         kConsumerWarps * 20 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int) +
-         (mlp ? (kMlpFragWords * 32 + kMlpBias + 3 + kConsumerWarps * 128) * 4 : 0);
+// With the learned closure (mlp = MLP_WARP or MLP_TCGEN05): its weight fragments, biases
+// and per-warp staging blocks; with MLP_TCGEN05 also the tcgen05 operands (sgs_umma.cuh).
+__host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, size_t elem, int mlp = 0,
+                                                   int groups = 1, int cpt = 1) {
+  return kSmemGuard + (size_t)stages * step_stage_bytes(L, elem, groups, cpt) + kSmemGuard + 16 +
+         16 * (size_t)stages + 2 * (size_t)L.ny * sizeof(double) +
+         (size_t)stages * rows_per_item(L.nx, cpt) * groups * sizeof(int2) +
+         kConsumerWarps * 24 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int) +
+         (mlp ? (kMlpFragWords * 32 + kMlpBias + 3 + kConsumerWarps * 128) * 4 : 0) +
+         (mlp == 2 ? kStepUmmaBytes : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -532,6 +555,14 @@ struct NearLink {
   uint32_t o1, o2;  // element offsets of p1, p2 (Layout::at)
   uint32_t d1, d2;  // their directions (the shifted codecs decode with w_d)
   double A, B;
+};
+// The compact table of the FP32-arithmetic kernels (16 bytes a link instead of 32): the
+// two populations of a link belong to directions d or opp(d), which share the weight
+// w_d, and A + B = 1 in every case, so the pulled deviation is
+//   f - w_d = c (A h1 + B h2) + (c - 1) w_d,   h = stored deviation, c = pending rescale.
+struct NearLinkF {
+  uint32_t o1, o2;
+  float A, B;
 };
 
 template <class S, int MODE>
@@ -575,14 +606,22 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, const void* fs
     else return f * corr;
   };
   Real v[19];
+  if constexpr (MODE == MODE_FAST) {
+    const float c = (float)corr, cw = c - 1.0f;
 #pragma unroll
-  for (int d = 0; d < 19; ++d) {
-    const NearLink lk = a.links[(long long)d * a.n_near + t];
-    const double p1 = S::f_of(fs[lk.o1], (int)lk.d1);
-    const double p2 = S::f_of(fs[lk.o2], (int)lk.d2);
-    const double val = lk.A * resc(p1) + lk.B * resc(p2);
-    if constexpr (MODE == MODE_FAST) v[d] = (float)(val - (double)wf_of(d));
-    else v[d] = val;
+    for (int d = 0; d < 19; ++d) {
+      const NearLinkF lk = a.links_f[(long long)d * a.n_near + t];
+      const float h1 = S::h_of(fs[lk.o1], d), h2 = S::h_of(fs[lk.o2], d);
+      v[d] = fmaf(c, fmaf(lk.A, h1, lk.B * h2), cw * wf_of(d));
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+      const NearLink lk = a.links[(long long)d * a.n_near + t];
+      const double p1 = S::f_of(fs[lk.o1], (int)lk.d1);
+      const double p2 = S::f_of(fs[lk.o2], (int)lk.d2);
+      v[d] = lk.A * resc(p1) + lk.B * resc(p2);
+    }
   }
   Mac mr, mx, my, mz;
   {
@@ -798,7 +837,7 @@ struct SegGeom {
   uint8_t cl;               // this lane's class byte
 };
 
-template <class S, class InletFn, bool MLP = false>
+template <class S, class InletFn, int MLP = MLP_NONE>
 __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __restrict__ fd, const SegGeom g,
                                              float tau0, float k_smag, float2 dec, InletFn inlet_u,
                                              const StepArgs& m,
@@ -810,10 +849,10 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
   T* const blk = fd + row * 19 * pitch;
   const bool own = g.active && g.flag != CELL_SOLID && !g.near && ix != 0 && ix != nx - 1;
   float r, ux, uy, uz;
-  if constexpr (MLP) {
+  if constexpr (MLP != MLP_NONE) {
     MlpRefs mr = *mlp;
     mr.wall_dist = (float)(g.cl >> 3);
-    collide_fast<S, true>(v, r, ux, uy, uz, tau0, k_smag, dec, &mr);  // v: storage domain
+    collide_fast<S, MLP>(v, r, ux, uy, uz, tau0, k_smag, dec, &mr);  // v: storage domain
   } else {
     collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag, dec);
   }
@@ -906,9 +945,160 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
   }
 }
 
-template <class S, int MODE, int P, bool MLP = false>
-__global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
+// Packed loads and stores of two adjacent cells (the first at an even element offset, so
+// the pair is 4- or 8-byte aligned) in the raw storage domain.
+template <class S>
+__device__ __forceinline__ float2 load_pair(const typename S::T* p) {
+  using T = typename S::T;
+  if constexpr (sizeof(T) == 4) {
+    return *reinterpret_cast<const float2*>(p);
+  } else if constexpr (std::is_same<T, __half>::value) {
+    return __half22float2(*reinterpret_cast<const __half2*>(p));
+  } else {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+  }
+}
+template <class S>
+__device__ __forceinline__ void store_pair(typename S::T* p, float2 v) {
+  using T = typename S::T;
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float2*>(p) = v;
+  } else if constexpr (std::is_same<T, __half>::value) {
+    *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
+  } else {
+    *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
+  }
+}
+
+// Geometry of a two-cells-per-thread segment: 64 cells of an x-row with an even cell
+// count, lane l holding cells x0 = cell_lo + 2 l and x0 + 1.
+struct PairGeom {
+  long long row;
+  int nx, ny, nz, pitch;
+  int iy, iz, x0;
+  bool active;           // both cells lie in the row (nx even: x0 < nx implies x0 + 1 < nx)
+  bool has_lo, has_hi;   // the segment holds cell 0 / cell nx-1 (warp-uniform)
+  bool wall_row, ground_no_slip, write_macro;
+  uint8_t c0, c1;        // class bytes of the two cells
+};
+
+// The consumer work of a two-cells-per-thread segment: the same per-cell semantics as
+// fast_segment (pull values in v, collision, inlet and outlet of the row, wall rows,
+// stores, density sum, macro outputs), with both row ends handled inside the thread that
+// holds them: the inlet cell 0 pairs with cell 1 whose density it takes, the outlet cell
+// nx-1 pairs with cell nx-2 whose post-collision values it blends
+// (lbmCpuReference.ts:323-373).  The outlet's sources (pre-wall values and moments of
+// nx-2) are parked in the warp's scratch row xo[24] and the row ends are written after
+// the cells' own stores, when the 19 pairs are no longer live.
+template <class S, class InletFn>
+__device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __restrict__ fd, const PairGeom g,
+                                             float tau0, float k_smag, float2 dec, InletFn inlet_u,
+                                             const StepArgs& m, float* xo, long long& my_sum, int& my_nan) {
+  using T = typename S::T;
+  constexpr float OS = S::kOutScale, OW = S::kOutW;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, pitch = g.pitch, x0 = g.x0;
+  const long long row = g.row;
+  T* const blk = fd + row * 19 * pitch;
+  float2 r, ux, uy, uz;
+  collide_fast2<S>(v, r, ux, uy, uz, tau0, k_smag, dec);  // v: storage domain
+  const int f0 = g.c0 & CLS_FLAG_MASK, f1 = g.c1 & CLS_FLAG_MASK;
+  const bool own0 = g.active && f0 != CELL_SOLID && !(g.c0 & CLS_NEAR) && x0 != 0;
+  const bool own1 = g.active && f1 != CELL_SOLID && !(g.c1 & CLS_NEAR) && x0 + 1 != nx - 1;
+  const bool lo = g.has_lo && x0 == 0, hi = g.has_hi && x0 == nx - 2;
+  if (hi) {  // the outlet's sources: cell nx-2 after the collision, before any wall condition
+#pragma unroll
+    for (int d = 0; d < 19; ++d) xo[slot_of(d)] = v[d].x;
+    xo[19] = r.x; xo[20] = ux.x; xo[21] = uy.x; xo[22] = uz.x;
+  }
+  if (g.wall_row) {  // floor, ceiling, then sides (:375-429), fluid cells only
+    if (g.iy == 0) {
+      if (g.ground_no_slip) { ux = f2(0.0f); uz = f2(0.0f); }
+      uy = f2(0.0f);
+    }
+    if (g.iy == ny - 1) uy = f2(0.0f);
+    if (nz > 4 && (g.iz == 0 || g.iz == nz - 1)) uz = f2(0.0f);
+    heq_pair<S>(v, r, ux, uy, uz);
+  }
+  T* out = blk + x0;
+  if (own0 && own1) {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) store_pair<S>(out + slot_of(d) * pitch, v[d]);
+  } else if (own0 || own1) {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+      if (own0) out[slot_of(d) * pitch] = S::store(v[d].x);
+      if (own1) out[slot_of(d) * pitch + 1] = S::store(v[d].y);
+    }
+  }
+  if (own0) {
+    if (r.x == r.x) my_sum += rho_fixed(r.x);
+    else my_nan = 1;
+  }
+  if (own1) {
+    if (r.y == r.y) my_sum += rho_fixed(r.y);
+    else my_nan = 1;
+  }
+  if (g.write_macro && g.active) {
+    const long long di = row * nx + x0;
+    if (f0 == CELL_SOLID) {  // solid macro (:173-179)
+      m.mux[di] = 0.0f; m.muy[di] = 0.0f; m.muz[di] = 0.0f; m.mrho[di] = 1.0f;
+    } else if (own0) {
+      m.mux[di] = ux.x; m.muy[di] = uy.x; m.muz[di] = uz.x; m.mrho[di] = r.x;
+    }
+    if (f1 == CELL_SOLID) {
+      m.mux[di + 1] = 0.0f; m.muy[di + 1] = 0.0f; m.muz[di + 1] = 0.0f; m.mrho[di + 1] = 1.0f;
+    } else if (own1) {
+      m.mux[di + 1] = ux.y; m.muy[di + 1] = uy.y; m.muz[di + 1] = uz.y; m.mrho[di + 1] = r.y;
+    }
+  }
+  if (lo) {
+    // inlet (:328-352) from the density of cell 1 (1 for a solid, :177; walls leave the
+    // density unchanged); a near-wall cell 1 defers it to the near-wall pass, a solid
+    // cell 0 has none
+    const bool solid1 = f1 == CELL_SOLID;
+    if (f0 != CELL_SOLID && !((g.c1 & CLS_NEAR) && !solid1)) {
+      const float ri = 0.85f * (solid1 ? 1.0f : r.y) + 0.15f;
+      const float2 ui = inlet_u(g.iy);
+#pragma unroll
+      for (int d = 0; d < 19; ++d)
+        blk[slot_of(d) * pitch] = S::store(fmaf(OS, heq32(d, ri, ui.x, ui.y, 0.0f), OW * wf_of(d)));
+      if (ri == ri) my_sum += rho_fixed(ri);
+      else my_nan = 1;
+      if (g.write_macro) {
+        const long long ic = row * nx;
+        m.mux[ic] = ui.x; m.muy[ic] = ui.y; m.muz[ic] = 0.0f; m.mrho[ic] = ri;
+      }
+    }
+  }
+  if (hi) {
+    // outlet (:354-371) from the post-collision, pre-wall cell nx-2, or from what fDst
+    // holds there when nx-2 is solid; a near-wall nx-2 defers it
+    const bool stale = f0 == CELL_SOLID;
+    if (f1 != CELL_SOLID && !((g.c0 & CLS_NEAR) && !stale)) {
+      const float ro = (stale ? 1.0f : xo[19]) * 0.85f + 0.15f;
+      const float mx = stale ? 0.0f : xo[20], my = stale ? 0.0f : xo[21], mz = stale ? 0.0f : xo[22];
+#pragma unroll
+      for (int d = 0; d < 19; ++d) {
+        const float prev = stale ? S::raw(blk[slot_of(d) * pitch + nx - 2]) : xo[slot_of(d)];
+        blk[slot_of(d) * pitch + nx - 1] =
+            S::store(0.75f * prev + 0.25f * fmaf(OS, heq32(d, ro, mx, my, mz), OW * wf_of(d)));
+      }
+      if (ro == ro) my_sum += rho_fixed(ro);
+      else my_nan = 1;
+      if (g.write_macro) {
+        const long long oc = row * nx + nx - 1;
+        m.mux[oc] = mx; m.muy[oc] = my; m.muz[oc] = mz; m.mrho[oc] = ro;
+      }
+    }
+  }
+}
+
+// CPT: consumer cells per thread, 1 or 2 (MODE_FAST without the closure, even nx; the
+// host chooses, pair_segment does the work).
+template <class S, int MODE, int P, int MLP = MLP_NONE, int CPT = 1>
+__global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP, CPT>())
     main_kernel(const __grid_constant__ StepArgs a) {
+  static_assert(CPT == 1 || (MODE == MODE_FAST && MLP == MLP_NONE), "two cells per thread: fast mode only");
   using T = typename S::T;
   using Real = typename std::conditional<MODE == MODE_FAST, float, double>::type;
   using Mac = typename MacroOf<T>::type;
@@ -916,13 +1106,14 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ long long red[kConsumerWarps + 2];
   __shared__ int nan_flag;
+  __shared__ long long s_first[8];  // dynamic deal: first row of the item in ring slot s (-1: none left)
 
   const Layout& L = a.L;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const int pitch = P ? P : L.pitch;
   const int S_ = a.stages;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int shift = row_shift(nx), span = row_span(nx), RY = rows_per_item(nx);
+  const int shift = row_shift(nx, CPT), span = row_span(nx, CPT), RY = rows_per_item(nx, CPT);
   const int wpr = span / 32;
   const long long rows = (long long)ny * nz;
   const int G = step_item_grouped<S, MODE, MLP>() && a.item_groups > 1 ? a.item_groups : 1;
@@ -944,18 +1135,26 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
   double* s_uxi = reinterpret_cast<double*>(empty + S_);
   double* s_uyi = s_uxi + ny;
   int2* s_row = reinterpret_cast<int2*>(s_uyi + ny);        // [S_][RYG] (iy, iz) of the slot's rows
-  float* s_xo = reinterpret_cast<float*>(s_row + S_ * RYG);  // [kConsumerWarps][20]
+  float* s_xo = reinterpret_cast<float*>(s_row + S_ * RYG);  // [kConsumerWarps][24]
   float4* s_dcw = reinterpret_cast<float4*>(
-      (reinterpret_cast<uintptr_t>(s_xo + kConsumerWarps * 20) + 15) & ~uintptr_t(15));  // [19]
+      (reinterpret_cast<uintptr_t>(s_xo + kConsumerWarps * 24) + 15) & ~uintptr_t(15));  // [19]
   int* s_dslot = reinterpret_cast<int*>(s_dcw + 19);                                     // [19]
   // learned closure: weight fragments, biases, one staging block per consumer warp
   uint32_t* s_mfrag = reinterpret_cast<uint32_t*>(s_dslot + 19);                          // [24 * 32]
   float* s_mbias = reinterpret_cast<float*>(s_mfrag + kMlpFragWords * 32);               // [65]
   uint32_t* s_mstage = reinterpret_cast<uint32_t*>(s_mbias + kMlpBias + 3);              // [8][128]
-  if constexpr (MLP) {
+  if constexpr (MLP != MLP_NONE) {
     for (int i = threadIdx.x; i < kMlpFragWords * 32; i += blockDim.x) s_mfrag[i] = a.mlp_frag[i];
     for (int i = threadIdx.x; i < kMlpBias; i += blockDim.x) s_mbias[i] = a.mlp_bias[i];
   }
+  // tcgen05 closure: the weight image, per group of four consumer warps its A operands
+  // and completion mbarrier, and the TMEM address slot (128-byte aligned region)
+  uint8_t* s_umma = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(s_mstage + kConsumerWarps * 128) + 127) & ~uintptr_t(127));
+  uint8_t* s_ub = s_umma;                                                   // weight image
+  uint8_t* s_ua = s_umma + kUmmaBBytes;                                     // [group] A1, A2
+  uint64_t* s_umbar = reinterpret_cast<uint64_t*>(s_ua + kStepUmmaGroups * (kStepUmmaA1 + kStepUmmaA2));
+  uint32_t* s_utmem = reinterpret_cast<uint32_t*>(s_umbar + kStepUmmaGroups);
 
   const T* __restrict__ fs = static_cast<const T*>(a.fsrc);
   T* __restrict__ fd = static_cast<T*>(a.fdst);
@@ -964,13 +1163,40 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
   // divide the 8 consumer warps (row spans of 96, 160, 192, 224 threads) the
   // remaining warps take no rows.
   const int n_cons = RY * wpr;
+  // the tcgen05 closure needs all 8 consumer warps busy on every item (two full groups);
+  // the host launches it only then, and a lattice where that does not hold steps nothing
+  // and reports an error instead of leaving a group barrier short of a warp
+  const bool groups_ok = MLP != MLP_TCGEN05 || n_cons == kConsumerWarps;
+  const int count = groups_ok ? my_count : 0;
+  // Dynamic deal: the producer takes items from the step's counter and publishes each
+  // item's first row with its slot; a slot holding -1 tells the consumers that no item is
+  // left.  Every cell's update reads only the source lattice, so the deal changes no result.
+  const bool dyn = a.dynamic_items && groups_ok;
+  const int cur_slot = a.step_index & 1;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S_; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], n_cons);
     }
     nan_flag = 0;
+    if (!groups_ok) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
     mbar_fence_init();
+  }
+  if constexpr (MLP == MLP_TCGEN05) {
+    for (int i = threadIdx.x; i < kUmmaBBytes / 16; i += blockDim.x)
+      reinterpret_cast<uint4*>(s_ub)[i] = a.mlp_umma[i];
+    if (warp < kConsumerWarps) {  // K padding of this thread's row of the input operand
+      const int g = warp >> 2, row = (warp & 3) * 32 + lane;
+      *reinterpret_cast<uint4*>(s_ua + g * (kStepUmmaA1 + kStepUmmaA2) + umma_off(row, 8, 16)) =
+          make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (threadIdx.x < kStepUmmaGroups) umma_mbar_init(smem_addr(&s_umbar[threadIdx.x]));
+    if (warp == 0) {
+      tmem_alloc(smem_addr(s_utmem), kStepUmmaTmemCols);
+      tmem_relinquish();
+    }
+    fence_async_smem();
+    tc_fence_before();
   }
   if (threadIdx.x < 19) {  // direction table of the lane-transposed row ends
     const int d = threadIdx.x;
@@ -999,6 +1225,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     s_uyi[i] = uyi;
   }
   __syncthreads();
+  if constexpr (MLP == MLP_TCGEN05) tc_fence_after();
   // Programmatic dependent launch: this CTA may have started while the previous kernel
   // of the stream was still finishing.  Everything above wrote only shared memory and
   // read only inputs the host copied in; wait for that kernel to complete and flush
@@ -1023,10 +1250,20 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     // ---------------- producer warp: lanes issue the copies of an item in parallel ----------------
     const uint32_t slot_bytes = (uint32_t)(pitch * sizeof(T));
     int issued = 0;
+    int end_slot = -1;  // the slot that took the dynamic deal's end mark
     int s = 0;
     uint32_t ph = 0;  // parity of the slot's current fill
     long long r0 = item_row0;  // first row of this CTA's j-th item
-    for (int j = 0; j < my_count; ++j, r0 += item_step) {
+    for (int j = 0;; ++j, r0 += item_step) {
+      long long k = 0;  // dynamic deal: this fill's item (-1: none left)
+      if (dyn) {
+        if (lane == 0) k = (long long)atomicAdd(&a.st->next_item[cur_slot], 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= n_items) k = -1;
+        else r0 = (reverse ? n_items - 1 - k : k) * RYG;
+      } else if (j >= count) {
+        break;
+      }
       if (j >= S_) {  // the slot's previous fill must have been consumed
         const bool ok = mbar_wait(&empty[s], ph ^ 1u, a.wait_limit);
         if (!__any_sync(0xffffffffu, ok)) {
@@ -1034,8 +1271,17 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
           break;
         }
       }
+      if (dyn && k < 0) {  // no items left: the consumers leave when they reach this slot
+        if (lane == 0) {
+          s_first[s] = -1;
+          mbar_arrive(&full[s]);
+        }
+        end_slot = s;
+        break;
+      }
       const int nr = (int)(rows - r0 < RYG ? rows - r0 : RYG);
       if (lane == 0) {
+        if (dyn) s_first[s] = r0;
         // row coordinates for the consumers, published by the arrive below
         for (int yy = 0; yy < nr; ++yy) {
           const int r = (int)(r0 + yy);
@@ -1065,9 +1311,12 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
     // No copy may still be in flight when the CTA exits: wait (bounded, always with the
     // full limit) for the last phase issued into every slot; completed phases return at
-    // once.
+    // once.  A slot that took the dynamic deal's end mark after its last fill had that
+    // fill consumed already (the producer waited for it), so it is skipped: its mbarrier
+    // has completed one more phase than the copies.
     if (lane == 0) {
       for (int k = 0; k < S_ && k < issued; ++k) {
+        if (k == end_slot) continue;
         const int last = k + ((issued - 1 - k) / S_) * S_;
         mbar_wait(&full[k], (uint32_t)((last / S_) & 1), kWaitLimit);
       }
@@ -1079,19 +1328,53 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     const float corrf = (float)corr;
     const float2 dec = make_float2(corrf * S::kRawScale, corrf - 1.0f);  // raw-moment decode
     const int ry = warp / wpr;
-    const int nchunks = (nx + shift + span - 1) / span;
+    const int nchunks = (nx + shift + span * CPT - 1) / (span * CPT);
     int my_nan = 0;
     int s = 0;
     uint32_t ph = 0;
     int seg = warp % wpr;  // the row-end segments rotate over the warps of a row
     long long row0 = item_row0 + ry;  // this warp's row of the item's first group
-    for (int j = 0; j < my_count; ++j, row0 += item_step) {
+    UmmaGroup ug{};
+    if constexpr (MLP == MLP_TCGEN05) {
+      const int g = warp >> 2;
+      const uint32_t ab = smem_addr(s_ua + g * (kStepUmmaA1 + kStepUmmaA2)), a2b = ab + (uint32_t)kStepUmmaA1;
+      const uint32_t bb = smem_addr(s_ub);
+      ug.a1 = s_ua + g * (kStepUmmaA1 + kStepUmmaA2);
+      ug.a2 = ug.a1 + kStepUmmaA1;
+      ug.dA1 = umma_smem_desc(ab, 128, 256);
+      ug.dA2lo = umma_smem_desc(a2b, 128, 512);
+      ug.dA2hi = umma_smem_desc(a2b + 256, 128, 512);
+      ug.dB1 = umma_smem_desc(bb + kUmmaB1, 128, 256);
+      ug.dB2lo = umma_smem_desc(bb + kUmmaB2, 128, 512);
+      ug.dB2hi = umma_smem_desc(bb + kUmmaB2 + 256, 128, 512);
+      ug.dB3lo = umma_smem_desc(bb + kUmmaB3, 128, 512);
+      ug.dB3hi = umma_smem_desc(bb + kUmmaB3 + 256, 128, 512);
+      ug.mbar = smem_addr(&s_umbar[g]);
+      ug.tmem = *s_utmem + (uint32_t)(g * 64);
+      ug.lane_addr = ug.tmem + ((uint32_t)((warp & 3) * 32) << 16);
+      ug.row = (warp & 3) * 32 + lane;
+      ug.bar_id = 1 + g;
+      ug.limit = kWaitLimit;
+      ug.issuer = (warp & 3) == 0 && lane == 0;
+    }
+    for (int j = 0; dyn || j < count; ++j, row0 += item_step) {
       {
         const bool ok = mbar_wait(&full[s], ph, a.wait_limit);
-        if (!__any_sync(0xffffffffu, ok)) {
+        if constexpr (MLP == MLP_TCGEN05) {
+          // the four warps of the group leave together (a failed ring wait or closure)
+          if (group_any(ug.bar_id, !__any_sync(0xffffffffu, ok) || ug.failed)) {
+            failed = true;
+            break;
+          }
+        } else if (!__any_sync(0xffffffffu, ok)) {
           failed = true;
           break;
         }
+      }
+      if (dyn) {  // the item the producer took for this slot
+        const long long first = s_first[s];
+        if (first < 0) break;
+        row0 = first + ry;
       }
       for (int gq = 0; gq < G; ++gq) {  // the item's row groups
         const long long row = row0 + (long long)gq * RY;
@@ -1106,6 +1389,40 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
         const uint8_t* sc = scls + (size_t)(s * RYG + gq * RY + ry) * pitch;
         const bool wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
 
+        if constexpr (CPT == 2) {
+          // two adjacent cells per lane: 64 cells per segment, no row shift (nx even)
+          auto inlet = [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); };
+          for (int c = 0; c < nchunks; ++c) {
+            const int cell_lo = c * span * 2 + seg * 64;  // first cell of lane 0
+            const int x0 = cell_lo + 2 * lane;
+            const bool active = row_ok && x0 < nx;
+            const int lx = active ? x0 : 0;  // lanes outside the row read cells 0 and 1
+            const uint32_t cls2 = *reinterpret_cast<const uint16_t*>(sc + lx);
+            float2 v[19];
+            // ---- pull-stream (lbmCpuReference.ts:189-231) from the staged rows: a pair
+            // load where the two sources are adjacent and aligned (c_x = 0) ----
+#pragma unroll
+            for (int d = 0; d < 19; ++d) {
+              const T* q = sp + slot_of(d) * pitch + lx;
+              if (cx_of(d) == 0) v[d] = load_pair<S>(q);
+              else v[d] = make_float2(S::raw(q[-cx_of(d)]), S::raw(q[1 - cx_of(d)]));
+            }
+            if (gq == G - 1 && c == nchunks - 1) {  // every value of this slot is in registers: release it
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&empty[s]);
+            }
+            PairGeom g;
+            g.row = row; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
+            g.iy = iy; g.iz = iz; g.x0 = x0; g.active = active;
+            g.has_lo = row_ok && cell_lo == 0;
+            g.has_hi = row_ok && cell_lo <= nx - 2 && nx - 2 < cell_lo + 64;
+            g.wall_row = wall_row; g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro;
+            g.c0 = (uint8_t)(cls2 & 0xffu);
+            g.c1 = (uint8_t)(cls2 >> 8);
+            pair_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a, s_xo + warp * 24, my_sum,
+                            my_nan);
+          }
+        } else
         for (int c = 0; c < nchunks; ++c) {
           const int cell_lo = c * span + seg * 32 - shift;  // cell of lane 0
           const int ix = cell_lo + lane;
@@ -1135,12 +1452,12 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
             g.row_ok = row_ok; g.active = active; g.near = near; g.wall_row = wall_row;
             g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro; g.cl = cl;
             auto inlet = [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); };
-            if constexpr (MLP) {
-              const MlpRefs mr{s_mfrag, s_mbias, s_mstage + warp * 128, a.mlp_nu0, 0.0f, lane};
-              fast_segment<S, decltype(inlet), true>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a,
-                                                     s_xo + warp * 20, s_dcw, s_dslot, lane, my_sum, my_nan, &mr);
+            if constexpr (MLP != MLP_NONE) {
+              const MlpRefs mr{s_mfrag, s_mbias, s_mstage + warp * 128, a.mlp_nu0, 0.0f, lane, &ug};
+              fast_segment<S, decltype(inlet), MLP>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a,
+                                                    s_xo + warp * 24, s_dcw, s_dslot, lane, my_sum, my_nan, &mr);
             } else {
-              fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a, s_xo + warp * 20, s_dcw,
+              fast_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a, s_xo + warp * 24, s_dcw,
                               s_dslot,
                               lane, my_sum, my_nan);
             }
@@ -1157,12 +1474,23 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     }
     if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
     if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
+    if constexpr (MLP == MLP_TCGEN05) {
+      if (ug.failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
+      // no tensor-core operation may still be running when the TMEM is freed: the
+      // issuing thread waits (full bound) for its last commit
+      if (ug.issuer && ug.issued > 0) umma_mbar_wait(ug.mbar, (uint32_t)((ug.issued - 1) & 1), kWaitLimit);
+    }
   }
 
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) my_sum += __shfl_down_sync(0xffffffffu, my_sum, o);
   if (lane == 0) red[warp] = my_sum;
+  if constexpr (MLP == MLP_TCGEN05) tc_fence_before();
   __syncthreads();
+  if constexpr (MLP == MLP_TCGEN05) {
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(*s_utmem, kStepUmmaTmemCols);
+  }
   const int slot = a.step_index & 1;
   __shared__ int is_last;
   if (threadIdx.x == 0) {
@@ -1195,6 +1523,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP>())
     // accumulators of the next step start from zero
     a.st->rho_sum[slot ^ 1] = 0ull;
     a.st->ticket[slot ^ 1] = 0u;
+    a.st->next_item[slot ^ 1] = 0u;
   }
 }
 

@@ -25,10 +25,10 @@ cudaError_t raise_smem_limit(K k) {
 
 // One time step: a single main_kernel launch.  Returns the number of launches in
 // *launches.
-template <class S, int MODE, int P, bool MLP = false>
+template <class S, int MODE, int P, int MLP = MLP_NONE, int CPT = 1>
 cudaError_t step_entry(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s, int* occ,
                        int* launches) {
-  auto k = main_kernel<S, MODE, P, MLP>;
+  auto k = main_kernel<S, MODE, P, MLP, CPT>;
   if (occ) {
     cudaError_t e = raise_smem_limit(k);
     if (e != cudaSuccess) return e;
@@ -54,16 +54,38 @@ cudaError_t step_entry(const StepArgs& a, dim3 block, unsigned grid, size_t smem
 // The FP32-arithmetic kernels are compiled for every row pitch up to 256 (multiples
 // of 32) with the pitch as a constant; other pitches and the double modes take the
 // run-time pitch.  With the learned closure (a.mlp_frag set): pitches 128 and 256, or
-// the run-time pitch.
+// the run-time pitch, as warp-level mma.sync tiles; with a.mlp_umma set as well, the
+// 128-cell tcgen05 tiles, for pitches 128 and 256 (rows of 97..256 cells: every item
+// keeps all 8 consumer warps busy, two full groups of four).
 template <class S, int MODE>
 cudaError_t step_dispatch(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s, int* occ,
                           int* launches) {
   if constexpr (MODE == MODE_FAST) {
+    if (a.mlp_frag && a.mlp_umma) {
+      switch (a.L.pitch) {
+        case 128: return step_entry<S, MODE, 128, MLP_TCGEN05>(a, block, grid, smem, s, occ, launches);
+        case 256: return step_entry<S, MODE, 256, MLP_TCGEN05>(a, block, grid, smem, s, occ, launches);
+        default: return cudaErrorInvalidValue;
+      }
+    }
     if (a.mlp_frag) {
       switch (a.L.pitch) {
-        case 128: return step_entry<S, MODE, 128, true>(a, block, grid, smem, s, occ, launches);
-        case 256: return step_entry<S, MODE, 256, true>(a, block, grid, smem, s, occ, launches);
-        default: return step_entry<S, MODE, 0, true>(a, block, grid, smem, s, occ, launches);
+        case 128: return step_entry<S, MODE, 128, MLP_WARP>(a, block, grid, smem, s, occ, launches);
+        case 256: return step_entry<S, MODE, 256, MLP_WARP>(a, block, grid, smem, s, occ, launches);
+        default: return step_entry<S, MODE, 0, MLP_WARP>(a, block, grid, smem, s, occ, launches);
+      }
+    }
+    if (a.cells_per_thread == 2) {  // two cells per thread (even nx)
+      switch (a.L.pitch) {
+        case 32: return step_entry<S, MODE, 32, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        case 64: return step_entry<S, MODE, 64, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        case 96: return step_entry<S, MODE, 96, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        case 128: return step_entry<S, MODE, 128, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        case 160: return step_entry<S, MODE, 160, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        case 192: return step_entry<S, MODE, 192, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        case 224: return step_entry<S, MODE, 224, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        case 256: return step_entry<S, MODE, 256, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
+        default: return step_entry<S, MODE, 0, MLP_NONE, 2>(a, block, grid, smem, s, occ, launches);
       }
     }
     switch (a.L.pitch) {

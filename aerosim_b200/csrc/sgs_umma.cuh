@@ -130,6 +130,102 @@ __device__ __forceinline__ void umma_store_hidden(uint8_t* A, int r, const float
     *reinterpret_cast<uint4*>(A + umma_off(r, 8 * g, 32)) = w;
   }
 }
+
+// ---- the closure inside the step kernel: 128-cell groups of four consumer warps -----
+// The step kernel's 8 consumer warps form two groups of four (warps 0-3 and 4-7); warp
+// w owns TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31, so the four warps of a group together
+// hold the 128 rows of one M = 128 tile: a group evaluates the network for its 128 cells
+// (one 32-cell segment per warp) with three tcgen05.mma layers issued by one thread.
+// Each group owns 64 TMEM columns (D1 and D3 at +0, D2 at +32; 128 per CTA), its A
+// operands and an mbarrier; the weight image is shared.  The four warps meet at a named
+// barrier before every layer; the barrier also reduces a failure flag (a timed-out
+// completion wait, or a ring wait that ran out before the segment), so that the warps of
+// a group always leave together and no barrier can wait for a warp that has left.
+constexpr int kStepUmmaGroups = 2;
+constexpr uint32_t kStepUmmaTmemCols = 128;  // power of two >= 32, per CTA
+constexpr size_t kStepUmmaA1 = 128 * 16 * 2, kStepUmmaA2 = 128 * 32 * 2;
+// shared memory of the tcgen05 closure: alignment slack, the weight image, the A
+// operands of each group, an mbarrier per group and the TMEM address slot
+constexpr size_t kStepUmmaBytes =
+    128 + kUmmaBBytes + kStepUmmaGroups * (kStepUmmaA1 + kStepUmmaA2) + 8 * kStepUmmaGroups + 8;
+
+struct UmmaGroup {
+  uint8_t* a1;  // 128 x 16 BF16 (inputs, K padded with zeros)
+  uint8_t* a2;  // 128 x 32 BF16 (hidden activations)
+  uint64_t dA1, dA2lo, dA2hi, dB1, dB2lo, dB2hi, dB3lo, dB3hi;  // operand descriptors
+  uint32_t mbar;       // shared address of the group's completion mbarrier
+  uint32_t tmem;       // the group's TMEM columns, lane 0
+  uint32_t lane_addr;  // the same, at this warp's 32 lanes
+  uint32_t phase;      // parity of the next completion
+  int issued;          // commits issued (issuing thread)
+  int row;             // this thread's cell = row of the tile
+  int bar_id;          // named barrier of the group (1 + group)
+  int limit;           // polls of a completion wait
+  bool issuer, failed;
+};
+
+// OR of v over the 128 threads of a group, at its named barrier.
+__device__ __forceinline__ bool group_any(int bar_id, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "barrier.cta.red.or.pred p, %2, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(bar_id)
+      : "memory");
+  return r != 0;
+}
+
+// nu_t / nu_0 of this thread's cell; all 128 threads of the group call it together.
+// Returns NaN when the group has failed (the caller then keeps the Smagorinsky tau and
+// leaves the item loop at its next group agreement).
+__device__ __forceinline__ float mlp_nut_umma(const float (&x)[kMlpIn], UmmaGroup& g, const float* bias) {
+  *reinterpret_cast<uint4*>(g.a1 + umma_off(g.row, 0, 16)) =
+      make_uint4(bf16x2_of(x[0], x[1]), bf16x2_of(x[2], x[3]), bf16x2_of(x[4], x[5]), bf16x2_of(x[6], x[7]));
+  constexpr uint32_t id32 = umma_idesc_bf16(kUmmaRows, 32), id16 = umma_idesc_bf16(kUmmaRows, 16);
+  bool ok = true;
+  float d[32];
+#pragma unroll 1
+  for (int layer = 0; layer < 3; ++layer) {
+    fence_async_smem();  // this thread's operand writes, visible to the tensor cores
+    tc_fence_before();
+    if (group_any(g.bar_id, g.failed || !ok)) {
+      g.failed = true;
+      return __int_as_float(0x7fc00000);
+    }
+    tc_fence_after();
+    if (g.issuer) {
+      if (layer == 0) {
+        umma_bf16(g.tmem, g.dA1, g.dB1, id32, 0u);
+      } else if (layer == 1) {
+        umma_bf16(g.tmem + 32, g.dA2lo, g.dB2lo, id32, 0u);
+        umma_bf16(g.tmem + 32, g.dA2hi, g.dB2hi, id32, 1u);
+      } else {
+        umma_bf16(g.tmem, g.dA2lo, g.dB3lo, id16, 0u);
+        umma_bf16(g.tmem, g.dA2hi, g.dB3hi, id16, 1u);
+      }
+      umma_commit(g.mbar);
+      ++g.issued;
+    }
+    // tcgen05.ld is warp-collective: a warp reads only when all its lanes saw the phase
+    ok = __all_sync(0xffffffffu, umma_mbar_wait(g.mbar, g.phase, g.limit));
+    g.phase ^= 1u;
+    if (ok) {
+      tc_fence_after();
+      if (layer < 2) {
+        tmem_ld32(g.lane_addr + (layer == 0 ? 0u : 32u), d);
+        umma_store_hidden(g.a2, g.row, d, bias + 32 * layer);
+      }
+    }
+  }
+  g.failed = g.failed || !ok;  // agreed on at the group's next barrier
+  if (!ok) return __int_as_float(0x7fc00000);
+  const float o = tmem_ld1(g.lane_addr) + bias[64];
+  tc_fence_before();
+  return softplus_f(o);
+}
 #endif
 
 }  // namespace aerosim

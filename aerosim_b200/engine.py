@@ -358,14 +358,26 @@ class LBMEngine:
                          C.byref(mq), C.byref(mo))
         return {"qValues": q, "omegaMag": om, "omegaVec": omv, "maxQ": mq.value, "maxOmega": mo.value}
 
-    def set_sgs_mlp(self, params) -> None:
+    def set_sgs_mlp(self, params, tensor_cores: str | None = None) -> None:
         """Learned SGS closure (aerosim_b200.sgs parameters) for the following steps;
-        None restores Smagorinsky."""
+        None restores Smagorinsky.  tensor_cores selects the in-kernel evaluation:
+        "mma_sync" (warp-level tiles), "tcgen05" (128-cell tiles, TMEM accumulators) or
+        None to keep the current choice."""
         if params is None:
             self._h.call("aerosim_set_sgs_mlp", None)
         else:
             p = np.ascontiguousarray(params, dtype=np.float32)
             self._h.call("aerosim_set_sgs_mlp", N.ptr(p, C.c_float))
+        if tensor_cores is not None:
+            self.set_sgs_path(tensor_cores)
+
+    def set_sgs_path(self, tensor_cores: str) -> str:
+        """Chooses the closure's tensor-core path ("default", "mma_sync", "tcgen05");
+        returns the path the next step runs ("mma_sync", "tcgen05", or "default" when
+        no closure is set)."""
+        used = C.c_int32()
+        self._h.call("aerosim_set_sgs_mlp_path", N.SGS_PATHS[tensor_cores], C.byref(used))
+        return {v: k for k, v in N.SGS_PATHS.items()}[used.value]
 
     def read_wall_distance(self) -> np.ndarray:
         info = self.voxel_info()

@@ -233,15 +233,20 @@ def run_ours(args) -> dict:
     wpath = os.path.join(ROOT, "aerosim_b200", "data", "sgs_mlp_ellipsoid.npz")
     if args.sgs_steps > 0 and os.path.exists(wpath):
         w = np.load(wpath)
-        e4, _ = _make_engine(case, "f32", dev)
-        e4.set_sgs_mlp(w["params"])
-        e4.step(args.warmup)
-        barrier_sync()
-        ms4, l4 = _timed_steps(e4, args.sgs_steps)
-        barrier_sync()
-        ms4 = max_over_ranks(ms4)
-        nan = e4.mass_stats()["hasNaN"]
-        e4.close()
+        in_step = {}
+        for path in ("tcgen05", "mma_sync"):  # the default path last: its figures head the entry
+            e4, _ = _make_engine(case, "f32", dev)
+            e4.set_sgs_mlp(w["params"])
+            used = e4.set_sgs_path(path)
+            e4.step(args.warmup)
+            barrier_sync()
+            ms4, l4 = _timed_steps(e4, args.sgs_steps)
+            barrier_sync()
+            ms4 = max_over_ranks(ms4)
+            nan = e4.mass_stats()["hasNaN"]
+            e4.close()
+            in_step[path] = {"path_used": used, "ms_per_step": ms4 / args.sgs_steps,
+                             "mlups": round(ws * cells * args.sgs_steps / (ms4 * 1e-3) / 1e6, 1), "nan": nan}
         meta = {}
         mpath = wpath.replace(".npz", ".json")
         if os.path.exists(mpath):
@@ -251,6 +256,7 @@ def run_ours(args) -> dict:
             "mlups": round(ws * cells * args.sgs_steps / (ms4 * 1e-3) / 1e6, 1), "ms_per_step": ms4 / args.sgs_steps,
             "vs_smagorinsky_time": round((ms4 / args.sgs_steps) / (ms / args.steps), 3), "gpu_launches": int(l4),
             "nan": nan, "inference": "BF16 mma.sync m16n8k16 tiles, FP32 accumulation, inside the step kernel",
+            "in_step_paths": in_step,
             "training": {k: meta[k] for k in ("fine", "coarse", "fine_cd_mean", "heldout_mse_mlp",
                                                "heldout_mse_smagorinsky", "coarse_smagorinsky", "coarse_mlp")
                          if k in meta},
@@ -266,7 +272,9 @@ def run_ours(args) -> dict:
     if args.cd_steps > 0:
         out["cd_err_vs_fp64"] = cd_vs_fp64(case, args.cd_steps, dev, blocks=10, steady=True)
     if args.cd_long_steps > 0:
-        out["cd_err_vs_fp64_long"] = cd_vs_fp64(case, args.cd_long_steps, dev, blocks=20, steady=False)
+        out["cd_err_vs_fp64_long"] = cd_vs_fp64(case, args.cd_long_steps, dev, blocks=20, steady=False,
+                                                precisions=tuple(args.cd_long_precisions.split(",")),
+                                                control=False)
 
     # ---- CPU baseline: the oracle on one core, bounded sample ----
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -311,7 +319,8 @@ def _cd_series(case, prec: str, steps: int, every: int, dev: int, perturb: float
             "mass_drift": m["meanRho"] - 1.0, "cumulative_rescale": m["cumulativeRescale"], "nan": m["hasNaN"]}
 
 
-def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True) -> dict:
+def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True,
+               precisions=("f32", "f16s", "bf16s"), control: bool = True) -> dict:
     """Cd / Cl / Cm of every storage mode against the FP64 GPU run (FP64 populations and
     arithmetic).  The flow at Re = 2e4 is unsteady and chaotic: runs that differ only in
     rounding follow each other for the first few thousand steps and then decorrelate.
@@ -326,8 +335,9 @@ def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True
     steady 64x32x32 sphere at Re = 100 (Cd averaged over steps 3500..4000) separates the
     storage error from the chaos."""
     every = 50
-    res = {p: _cd_series(case, p, steps, every, dev) for p in ("f64", "f32", "f16s", "bf16s")}
-    res["f64_perturbed"] = _cd_series(case, "f64", steps, every, dev, perturb=2.0 ** -11)
+    res = {p: _cd_series(case, p, steps, every, dev) for p in ("f64", *precisions)}
+    if control:
+        res["f64_perturbed"] = _cd_series(case, "f64", steps, every, dev, perturb=2.0 ** -11)
 
     def late(x, st):
         sel = x[st > steps // 2]
@@ -344,7 +354,7 @@ def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True
                        "mass_drift": ref["mass_drift"], "cumulative_rescale": ref["cumulative_rescale"],
                        "nan": ref["nan"]}}
     scale = float(np.mean(np.abs(ref["cd"][early]))) if early.any() else float("nan")
-    for p in ("f32", "f16s", "bf16s", "f64_perturbed"):
+    for p in (*precisions, *(("f64_perturbed",) if control else ())):
         r = res[p]
         lm = late(r["cd"], r["step"])
         d = {"dcd_mean_rel_late": abs(lm[0] - ref_late[0]) / abs(ref_late[0]),
@@ -358,8 +368,9 @@ def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True
             dev_idx = np.nonzero(np.abs(r["cd"] - ref["cd"]) > 0.01 * scale)[0]
             d["first_step_dcd_gt_1pct"] = int(r["step"][dev_idx[0]]) if dev_idx.size else None
         summary[p] = d
-    summary["f64_perturbed"]["perturbation"] = "initial deviations from the rest weights x (1 + 2^-11 xi), " \
-                                               "xi uniform in [-1, 1]"
+    if control:
+        summary["f64_perturbed"]["perturbation"] = "initial deviations from the rest weights x (1 + 2^-11 xi), " \
+                                                   "xi uniform in [-1, 1]"
     if steady:
         from aerosim_b200 import cases
         sph = cases.sphere_64x32x32()
@@ -522,6 +533,8 @@ def main():
     ap.add_argument("--cd-steps", type=int, default=20000, help="steps of the FP64-oracle Cd comparison (0: skip)")
     ap.add_argument("--cd-long-steps", type=int, default=0,
                     help="steps of a second, long FP64-oracle Cd comparison for late-window means (0: skip)")
+    ap.add_argument("--cd-long-precisions", default="f16s,bf16s,f32",
+                    help="storage modes of the long comparison")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--sgs-steps", type=int, default=2000,
                     help="steps of the 256x128x128 case with the learned closure (0: skip)")

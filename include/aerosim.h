@@ -266,6 +266,16 @@ int aerosim_mlp_train(float* params, const float* X, const float* Y, int64_t n, 
 /* params: the closure's weights for this engine's steps, NULL for Smagorinsky.  The
  * F32, F16S and BF16S precisions use it (near-wall Bouzidi cells keep Smagorinsky). */
 int aerosim_set_sgs_mlp(aerosim_engine* h, const float* params);
+/* Tensor-core path of the closure inside the step kernel.  AEROSIM_SGS_PATH_WARP: each
+ * warp evaluates its 32 cells as BF16 mma.sync m16n8k16 tiles in registers (the default);
+ * AEROSIM_SGS_PATH_TCGEN05: four consumer warps form one 128-cell tile, one thread issues
+ * each layer as tcgen05.mma (M 128) with BF16 operands in shared memory and FP32
+ * accumulators in tensor memory -- lattices with a row pitch of 128 or 256 (nx 97..256);
+ * other lattices keep the warp path.  *in_use (may be NULL) receives the path the next
+ * step will run (AEROSIM_SGS_PATH_DEFAULT when no closure is set).  No reference
+ * counterpart. */
+enum aerosim_sgs_path { AEROSIM_SGS_PATH_DEFAULT = 0, AEROSIM_SGS_PATH_WARP = 1, AEROSIM_SGS_PATH_TCGEN05 = 2 };
+int aerosim_set_sgs_mlp_path(aerosim_engine* h, int32_t path, int32_t* in_use);
 /* Euclidean distance (cells) of every cell centre to the nearest solid cell centre
  * (jump flooding), float[nx*ny*nz]. */
 int aerosim_read_wall_distance(aerosim_engine* h, float* out);

@@ -53,6 +53,31 @@ def test_step_wait_timeout_reports_device_error_and_recovers(gpu_engine_cls, pre
     e.close()
 
 
+def test_closure_tcgen05_groups_leave_together_on_timeout(gpu_engine_cls):
+    """With the closure on tcgen05 tiles, the four warps of a group agree on a failed ring
+    wait at a named barrier and leave together (none waits for a warp that has left);
+    the TMEM is released and the engine recovers."""
+    from aerosim_b200 import sgs
+    case = cases.scaled_ellipsoid(128, 32, 32)
+    fresh = _engine(case, "f32")
+    fresh.set_sgs_mlp(sgs.init_params(2), tensor_cores="tcgen05")
+    fresh.step(10)
+    f_fresh = fresh.read_populations()
+    fresh.close()
+    e = _engine(case, "f32")
+    e.set_sgs_mlp(sgs.init_params(2), tensor_cores="tcgen05")
+    assert e.set_sgs_path("tcgen05") == "tcgen05"
+    e.set_pipeline_wait_limit(0)
+    with pytest.raises(AerosimError) as err:
+        e.step(3)
+    assert err.value.code == N.ERR_DEVICE
+    e.set_pipeline_wait_limit(-1)
+    e.reset_flow()
+    e.step(10)
+    assert np.array_equal(e.read_populations().view(np.uint32), f_fresh.view(np.uint32))
+    e.close()
+
+
 def test_batch_wait_timeout_reports_device_error_and_recovers(gpu_engine_cls):
     def case(nx, r):
         c = meshes.lattice_center(nx, 24, 24, 1.0, (nx / 3, 11.5, 11.5))

@@ -164,3 +164,83 @@ def test_trained_closure_beats_smagorinsky_on_held_out_samples():
     print(f"held-out MSE of nu_t/nu_0: closure {mse_mlp:.4g}, Smagorinsky {mse_smag:.4g}, zero {mse_zero:.4g}")
     assert mse_mlp < 0.9 * mse_smag, (mse_mlp, mse_smag)
     assert mse_mlp < mse_zero, (mse_mlp, mse_zero)
+
+
+def _closure_params(seed):
+    """A network with a non-trivial response over the flow's features (larger weights
+    than the initialisation, output around nu_t / nu_0 ~ 1)."""
+    p = sgs.init_params(seed)
+    p[: 32 * 8] *= 4.0
+    return p
+
+
+@pytest.mark.parametrize("dims", [(128, 64, 64), (256, 32, 32), (100, 24, 20), (120, 15, 9)])
+def test_in_step_closure_tcgen05_tiles_match_warp_tiles(dims):
+    """The closure inside the step kernel as 128-cell tcgen05 tiles (four consumer warps,
+    one thread issuing each layer, TMEM accumulators) steps like the warp-level mma.sync
+    tiles: the same BF16 network with FP32 accumulation in another summation order, so
+    populations agree within 1e-5 relative after 60 steps.  Row pitches 128 and 256, one
+    or two rows per work item, an odd row count (the last item's second row is empty)."""
+    nx, ny, nz = dims
+    case = cases.scaled_ellipsoid(nx, ny, nz)
+    p = _closure_params(21)
+    out = {}
+    for path in ("mma_sync", "tcgen05"):
+        e = LBMEngine(0)
+        e.voxelize(case.mesh, None, case.tunnel, {"nx": nx, "ny": ny, "nz": nz},
+                   {"uInletLattice": case.u_inlet, "nuLattice": case.nu, "smagorinskyCs": case.cs,
+                    "precision": "f32"})
+        e.set_sgs_mlp(p)
+        assert e.set_sgs_path(path) == path
+        e.step(60)
+        m = e.mass_stats()
+        assert not m["hasNaN"]
+        out[path] = (e.read_populations().astype(np.float64), e.read_macro(), e.read_voxel_grid().cellFlags)
+        e.close()
+    fw, mw, flags = out["mma_sync"]
+    ft, mt, _ = out["tcgen05"]
+    rel = np.abs(ft - fw) / np.maximum(np.abs(fw), 1e-12)
+    rel[np.tile(flags == 1, 19)] = 0.0
+    assert rel.max() <= 1e-5, rel.max()
+    for k in ("ux", "uy", "uz", "rho"):
+        assert np.abs(mt[k] - mw[k]).max() <= 1e-5, k
+
+
+def test_in_step_closure_tcgen05_constant_network_equals_plain_viscosity():
+    """W3 = 0 and softplus(b3) = r: the tcgen05 tiles must return r for every cell, so the
+    run equals the plain method at nu_0 (1 + r) (empty tunnel, as the warp-path test)."""
+    case = cases.Case("empty", 128, 32, 32, (np.zeros((0, 3), np.float32), None), 0.05, 0.004, 0.1, 200)
+    r = 0.5
+    p = sgs.init_params(0)
+    p[-33:-1] = 0.0
+    p[-1] = np.log(np.expm1(r))
+    out = []
+    for closure in (True, False):
+        e = LBMEngine(0)
+        nu = case.nu * (1.0 + r) if not closure else case.nu
+        e.voxelize(case.mesh, None, case.tunnel, {"nx": case.nx, "ny": case.ny, "nz": case.nz},
+                   {"uInletLattice": case.u_inlet, "nuLattice": nu, "smagorinskyCs": 0.1 if closure else 0.0,
+                    "precision": "f32"})
+        if closure:
+            e.set_sgs_mlp(p, tensor_cores="tcgen05")
+            assert e.set_sgs_path("tcgen05") == "tcgen05"
+        e.step(200)
+        out.append(e.read_populations().astype(np.float64))
+        e.close()
+    rel = np.abs(out[0] - out[1]) / np.maximum(np.abs(out[1]), 1e-12)
+    assert rel.max() <= 1e-4, rel.max()
+
+
+def test_in_step_closure_path_selection():
+    """tcgen05 tiles need every work item to keep the 8 consumer warps busy (row pitch
+    128 or 256); other lattices keep the warp-level tiles."""
+    for (nx, expect) in ((64, "mma_sync"), (160, "mma_sync"), (128, "tcgen05"), (250, "tcgen05")):
+        case = cases.scaled_ellipsoid(nx, 32, 32)
+        e = LBMEngine(0)
+        e.voxelize(case.mesh, None, case.tunnel, {"nx": nx, "ny": 32, "nz": 32}, {"precision": "f32"})
+        assert e.set_sgs_path("tcgen05") == "default"  # no closure set yet
+        e.set_sgs_mlp(sgs.init_params(1))
+        assert e.set_sgs_path("tcgen05") == expect, nx
+        assert e.set_sgs_path("mma_sync") == "mma_sync"
+        e.step(3)
+        e.close()
