@@ -41,7 +41,7 @@ struct aerosim_engine {
   int stages = 3;
   int item_groups = 1;  // row groups per work item of the step kernel
   int cells_per_thread = 1;  // consumer cells per thread of the step kernel (1 or 2)
-  int dynamic_items = 0;     // work items from a device counter (1) or dealt round-robin (0)
+  int dynamic_items = 1;     // work items from a device counter (1) or dealt round-robin (0)
   int occupancy = 0;
   int num_sms = 148;
   float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
@@ -162,11 +162,13 @@ int configure_step(aerosim_engine* h) {
   const int mlp = h->mlp_frag ? (dummy.mlp_umma ? 2 : 1) : 0;
   const bool half = h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S;
   const bool fast = half || h->cfg.precision == AEROSIM_PREC_F32;
-  // two cells per consumer thread (packed FP32 pairs) for the 16-bit storage kernels
-  // without the closure on rows of an even cell count; AEROSIM_CELLS_PER_THREAD (1 or 2)
-  // overrides the choice for any fast-mode lattice that allows it
+  // two cells per consumer thread (packed FP32 pairs) without the closure on rows of an
+  // even cell count; AEROSIM_CELLS_PER_THREAD (1 or 2) overrides the choice for any
+  // fast-mode lattice that allows it
   const bool pairs_fit = !mlp && L.nx % 2 == 0 && L.nx >= 4;
-  int cpt = (half && pairs_fit) ? 2 : 1;
+  // FP32 storage: two cells per thread (103.9 vs 108.8 us per step at 256x128x128 with the
+  // dynamic deal); the 16-bit storage kernels measured slower with pairs (84.7 vs 80.5 us)
+  int cpt = (h->cfg.precision == AEROSIM_PREC_F32 && pairs_fit) ? 2 : 1;
   if (const char* cenv = getenv("AEROSIM_CELLS_PER_THREAD")) {
     const int want = atoi(cenv);
     if (want == 1) cpt = 1;
@@ -197,7 +199,8 @@ int configure_step(aerosim_engine* h) {
   h->smem = step_smem_bytes(L, best_s, eb, mlp, groups, cpt);
   h->item_groups = groups;
   h->cells_per_thread = cpt;
-  // AEROSIM_DYNAMIC_ITEMS (0 or 1) overrides the deal of the work items
+  // work items from the step's counter (108.8 vs 115.8 us FP32 with one cell per thread):
+  // AEROSIM_DYNAMIC_ITEMS (0 or 1) overrides the default deal
   if (const char* denv = getenv("AEROSIM_DYNAMIC_ITEMS")) h->dynamic_items = atoi(denv) ? 1 : 0;
   // the occupancy of the chosen configuration
   CU(h, launch_step(h->cfg.precision, dummy, block, 0, h->smem, h->stream, &best_occ, nullptr));
@@ -1569,6 +1572,10 @@ int aerosim_batch_autotune(aerosim_batch* b, int32_t steps_per_trial, aerosim_ba
   if (!b) return bfail(AEROSIM_ERR_ARG, "batch_autotune: NULL batch");
   if (steps_per_trial < 1) return bfail(AEROSIM_ERR_ARG, "batch_autotune: steps_per_trial must be positive");
   BCU(cudaSetDevice(b->device));
+  // trials start from fresh flows and a cleared error flag (a step that timed out before
+  // the autotune leaves the flag set until the batch is reset)
+  int rc0 = batch_reset(b);
+  if (rc0) return rc0;
   const aerosim_batch_tuning keep = b->tune;
   aerosim_batch_tuning best = keep;
   best.ms_per_step = 1e300;

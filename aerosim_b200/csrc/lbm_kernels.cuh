@@ -856,7 +856,10 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
   } else {
     collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag, dec);
   }
-  if (g.row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
+  // The row-end and wall-row conditions hold for a whole warp or for none of it; tested
+  // through a vote, so that the compiler branches around the blocks (the warps without a
+  // row end skip them) instead of predicating them in every warp.
+  if (__any_sync(0xffffffffu, g.row_ok && cell_lo <= 0 && 1 <= cell_lo + 31)) {
     // inlet (:328-352): density of ix = 1 (1 for a solid, :177); a near-wall ix = 1
     // defers the inlet to the near-wall pass, a solid ix = 0 has none
     const int c0 = __shfl_sync(0xffffffffu, (int)g.cl, -cell_lo);
@@ -881,7 +884,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
       }
     }
   }
-  if (g.row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31) {
+  if (__any_sync(0xffffffffu, g.row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31)) {
     // outlet (:354-371) from the post-collision, pre-wall cell nx-2, or from what fDst
     // holds there when nx-2 is solid; a near-wall nx-2 defers it
     const int src = nx - 2 - cell_lo;
@@ -918,7 +921,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
       }
     }
   }
-  if (g.wall_row) {  // floor, ceiling, then sides (:375-429), fluid cells only
+  if (__any_sync(0xffffffffu, g.wall_row)) {  // floor, ceiling, then sides (:375-429), fluid cells only
     if (g.iy == 0) {
       if (g.ground_no_slip) { ux = 0.0f; uz = 0.0f; }
       uy = 0.0f;
