@@ -856,10 +856,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
   } else {
     collide_fast<S>(v, r, ux, uy, uz, tau0, k_smag, dec);
   }
-  // The row-end and wall-row conditions hold for a whole warp or for none of it; tested
-  // through a vote, so that the compiler branches around the blocks (the warps without a
-  // row end skip them) instead of predicating them in every warp.
-  if (__any_sync(0xffffffffu, g.row_ok && cell_lo <= 0 && 1 <= cell_lo + 31)) {
+  if (g.row_ok && cell_lo <= 0 && 1 <= cell_lo + 31) {
     // inlet (:328-352): density of ix = 1 (1 for a solid, :177); a near-wall ix = 1
     // defers the inlet to the near-wall pass, a solid ix = 0 has none
     const int c0 = __shfl_sync(0xffffffffu, (int)g.cl, -cell_lo);
@@ -884,7 +881,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
       }
     }
   }
-  if (__any_sync(0xffffffffu, g.row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31)) {
+  if (g.row_ok && cell_lo <= nx - 2 && nx - 1 <= cell_lo + 31) {
     // outlet (:354-371) from the post-collision, pre-wall cell nx-2, or from what fDst
     // holds there when nx-2 is solid; a near-wall nx-2 defers it
     const int src = nx - 2 - cell_lo;
@@ -921,7 +918,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
       }
     }
   }
-  if (__any_sync(0xffffffffu, g.wall_row)) {  // floor, ceiling, then sides (:375-429), fluid cells only
+  if (g.wall_row) {  // floor, ceiling, then sides (:375-429), fluid cells only
     if (g.iy == 0) {
       if (g.ground_no_slip) { ux = 0.0f; uz = 0.0f; }
       uy = 0.0f;
@@ -979,6 +976,7 @@ struct PairGeom {
   long long row;
   int nx, ny, nz, pitch;
   int iy, iz, x0;
+  int cell_lo;           // first cell of lane 0
   bool active;           // both cells lie in the row (nx even: x0 < nx implies x0 + 1 < nx)
   bool has_lo, has_hi;   // the segment holds cell 0 / cell nx-1 (warp-uniform)
   bool wall_row, ground_no_slip, write_macro;
@@ -987,16 +985,18 @@ struct PairGeom {
 
 // The consumer work of a two-cells-per-thread segment: the same per-cell semantics as
 // fast_segment (pull values in v, collision, inlet and outlet of the row, wall rows,
-// stores, density sum, macro outputs), with both row ends handled inside the thread that
-// holds them: the inlet cell 0 pairs with cell 1 whose density it takes, the outlet cell
-// nx-1 pairs with cell nx-2 whose post-collision values it blends
-// (lbmCpuReference.ts:323-373).  The outlet's sources (pre-wall values and moments of
-// nx-2) are parked in the warp's scratch row xo[24] and the row ends are written after
-// the cells' own stores, when the 19 pairs are no longer live.
+// stores, density sum, macro outputs).  The thread that holds cell 0 holds cell 1 too, and
+// the thread that holds cell nx-1 holds nx-2, so the boundary conditions' sources
+// (lbmCpuReference.ts:323-373) sit with the row end: the outlet's (cell nx-2 after the
+// collision, before any wall condition: 19 values and the moments) are parked in the
+// warp's scratch row xo[24].  After the cells' own stores the warp holding a row end writes
+// it lane-transposed (lane d writes direction d), so the row-end work is one equilibrium
+// per lane and not 19 per thread, whether the compiler branches around it or predicates it.
 template <class S, class InletFn>
 __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __restrict__ fd, const PairGeom g,
                                              float tau0, float k_smag, float2 dec, InletFn inlet_u,
-                                             const StepArgs& m, float* xo, long long& my_sum, int& my_nan) {
+                                             const StepArgs& m, float* xo, const float4* s_dcw,
+                                             const int* s_dslot, int lane, long long& my_sum, int& my_nan) {
   using T = typename S::T;
   constexpr float OS = S::kOutScale, OW = S::kOutW;
   const int nx = g.nx, ny = g.ny, nz = g.nz, pitch = g.pitch, x0 = g.x0;
@@ -1007,8 +1007,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
   const int f0 = g.c0 & CLS_FLAG_MASK, f1 = g.c1 & CLS_FLAG_MASK;
   const bool own0 = g.active && f0 != CELL_SOLID && !(g.c0 & CLS_NEAR) && x0 != 0;
   const bool own1 = g.active && f1 != CELL_SOLID && !(g.c1 & CLS_NEAR) && x0 + 1 != nx - 1;
-  const bool lo = g.has_lo && x0 == 0, hi = g.has_hi && x0 == nx - 2;
-  if (hi) {  // the outlet's sources: cell nx-2 after the collision, before any wall condition
+  if (g.has_hi && x0 == nx - 2) {  // the outlet's sources
 #pragma unroll
     for (int d = 0; d < 19; ++d) xo[slot_of(d)] = v[d].x;
     xo[19] = r.x; xo[20] = ux.x; xo[21] = uy.x; xo[22] = uz.x;
@@ -1054,43 +1053,55 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
       m.mux[di + 1] = ux.y; m.muy[di + 1] = uy.y; m.muz[di + 1] = uz.y; m.mrho[di + 1] = r.y;
     }
   }
-  if (lo) {
-    // inlet (:328-352) from the density of cell 1 (1 for a solid, :177; walls leave the
-    // density unchanged); a near-wall cell 1 defers it to the near-wall pass, a solid
-    // cell 0 has none
-    const bool solid1 = f1 == CELL_SOLID;
-    if (f0 != CELL_SOLID && !((g.c1 & CLS_NEAR) && !solid1)) {
-      const float ri = 0.85f * (solid1 ? 1.0f : r.y) + 0.15f;
+  if (g.has_lo) {
+    // inlet (:328-352) from the density of cell 1 (1 for a solid, :177; the walls leave
+    // the density as it is), both held by lane 0; a near-wall cell 1 defers it to the
+    // near-wall pass, a solid cell 0 has none
+    const int c0 = __shfl_sync(0xffffffffu, (int)g.c0, 0), c1 = __shfl_sync(0xffffffffu, (int)g.c1, 0);
+    const float r1 = __shfl_sync(0xffffffffu, r.y, 0);
+    const bool solid1 = (c1 & CLS_FLAG_MASK) == CELL_SOLID;
+    if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
+      const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
       const float2 ui = inlet_u(g.iy);
-#pragma unroll
-      for (int d = 0; d < 19; ++d)
-        blk[slot_of(d) * pitch] = S::store(fmaf(OS, heq32(d, ri, ui.x, ui.y, 0.0f), OW * wf_of(d)));
-      if (ri == ri) my_sum += rho_fixed(ri);
-      else my_nan = 1;
-      if (g.write_macro) {
-        const long long ic = row * nx;
-        m.mux[ic] = ui.x; m.muy[ic] = ui.y; m.muz[ic] = 0.0f; m.mrho[ic] = ri;
+      if (lane < 19) {
+        const float4 cw = s_dcw[lane];
+        blk[s_dslot[lane] * pitch] = S::store(fmaf(OS, heq_lane(cw, ri, ui.x, ui.y, 0.0f), OW * cw.w));
+      }
+      if (lane == 0) {
+        if (ri == ri) my_sum += rho_fixed(ri);
+        else my_nan = 1;
+        if (g.write_macro) {
+          const long long ic = row * nx;
+          m.mux[ic] = ui.x; m.muy[ic] = ui.y; m.muz[ic] = 0.0f; m.mrho[ic] = ri;
+        }
       }
     }
   }
-  if (hi) {
-    // outlet (:354-371) from the post-collision, pre-wall cell nx-2, or from what fDst
-    // holds there when nx-2 is solid; a near-wall nx-2 defers it
-    const bool stale = f0 == CELL_SOLID;
-    if (f1 != CELL_SOLID && !((g.c0 & CLS_NEAR) && !stale)) {
+  if (g.has_hi) {
+    // outlet (:354-371) from the parked cell nx-2, or from what fDst holds there when
+    // nx-2 is solid; a near-wall nx-2 defers it
+    const int src = (nx - 2 - g.cell_lo) >> 1;
+    const int c2 = __shfl_sync(0xffffffffu, (int)g.c0, src), c3 = __shfl_sync(0xffffffffu, (int)g.c1, src);
+    const bool stale = (c2 & CLS_FLAG_MASK) == CELL_SOLID;
+    if ((c3 & CLS_FLAG_MASK) != CELL_SOLID && !((c2 & CLS_NEAR) && !stale)) {
+      __syncwarp();
       const float ro = (stale ? 1.0f : xo[19]) * 0.85f + 0.15f;
       const float mx = stale ? 0.0f : xo[20], my = stale ? 0.0f : xo[21], mz = stale ? 0.0f : xo[22];
-#pragma unroll
-      for (int d = 0; d < 19; ++d) {
-        const float prev = stale ? S::raw(blk[slot_of(d) * pitch + nx - 2]) : xo[slot_of(d)];
-        blk[slot_of(d) * pitch + nx - 1] =
-            S::store(0.75f * prev + 0.25f * fmaf(OS, heq32(d, ro, mx, my, mz), OW * wf_of(d)));
+      if (lane < 19) {
+        const float4 cw = s_dcw[lane];
+        const int sl = s_dslot[lane];
+        const float prev = stale ? S::raw(blk[sl * pitch + nx - 2]) : xo[sl];
+        blk[sl * pitch + nx - 1] =
+            S::store(0.75f * prev + 0.25f * fmaf(OS, heq_lane(cw, ro, mx, my, mz), OW * cw.w));
       }
-      if (ro == ro) my_sum += rho_fixed(ro);
-      else my_nan = 1;
-      if (g.write_macro) {
-        const long long oc = row * nx + nx - 1;
-        m.mux[oc] = mx; m.muy[oc] = my; m.muz[oc] = mz; m.mrho[oc] = ro;
+      __syncwarp();  // the scratch row is free for the next segment
+      if (lane == 0) {
+        if (ro == ro) my_sum += rho_fixed(ro);
+        else my_nan = 1;
+        if (g.write_macro) {
+          const long long oc = row * nx + nx - 1;
+          m.mux[oc] = mx; m.muy[oc] = my; m.muz[oc] = mz; m.mrho[oc] = ro;
+        }
       }
     }
   }
@@ -1416,14 +1427,14 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP, CP
             }
             PairGeom g;
             g.row = row; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
-            g.iy = iy; g.iz = iz; g.x0 = x0; g.active = active;
+            g.iy = iy; g.iz = iz; g.x0 = x0; g.cell_lo = cell_lo; g.active = active;
             g.has_lo = row_ok && cell_lo == 0;
             g.has_hi = row_ok && cell_lo <= nx - 2 && nx - 2 < cell_lo + 64;
             g.wall_row = wall_row; g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro;
             g.c0 = (uint8_t)(cls2 & 0xffu);
             g.c1 = (uint8_t)(cls2 >> 8);
-            pair_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a, s_xo + warp * 24, my_sum,
-                            my_nan);
+            pair_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a, s_xo + warp * 24, s_dcw,
+                            s_dslot, lane, my_sum, my_nan);
           }
         } else
         for (int c = 0; c < nchunks; ++c) {
