@@ -166,9 +166,9 @@ int configure_step(aerosim_engine* h) {
   // even cell count; AEROSIM_CELLS_PER_THREAD (1 or 2) overrides the choice for any
   // fast-mode lattice that allows it
   const bool pairs_fit = !mlp && L.nx % 2 == 0 && L.nx >= 4;
-  // FP32 storage: two cells per thread (103.9 vs 108.8 us per step at 256x128x128 with the
-  // dynamic deal); the 16-bit storage kernels measured slower with pairs (84.7 vs 80.5 us)
-  int cpt = (h->cfg.precision == AEROSIM_PREC_F32 && pairs_fit) ? 2 : 1;
+  // measured at 256x128x128 with the dynamic deal: FP32 103.5 vs 108.4 us per step, FP16S
+  // 76.0 vs 80.6, BF16S 75.6 vs 80.4 (two cells per thread vs one)
+  int cpt = (fast && pairs_fit) ? 2 : 1;
   if (const char* cenv = getenv("AEROSIM_CELLS_PER_THREAD")) {
     const int want = atoi(cenv);
     if (want == 1) cpt = 1;
@@ -176,7 +176,11 @@ int configure_step(aerosim_engine* h) {
   }
   dummy.cells_per_thread = cpt;
   const bool grouped = !mlp && half;
-  const int groups = grouped ? item_groups_for(L.nx, cpt) : 1;
+  int groups = grouped ? item_groups_for(L.nx, cpt) : 1;
+  if (const char* genv = getenv("AEROSIM_ITEM_GROUPS")) {  // override of the row groups per item (1..4)
+    const int want = atoi(genv);
+    if (grouped && want >= 1 && want <= 4) groups = want;
+  }
   const char* env = getenv("AEROSIM_STAGES");
   const int forced = env ? atoi(env) : 0;
   int best_s = 0, best_occ = 0;
