@@ -15,6 +15,7 @@
 #include "engine_internal.h"
 #include "lbm_kernels.cuh"
 #include "lbm_batch.cuh"
+#include "lbm_direct.cuh"
 #include "sgs_mlp.cuh"
 
 using namespace aerosim;
@@ -42,6 +43,7 @@ struct aerosim_engine {
   int item_groups = 1;  // row groups per work item of the step kernel
   int cells_per_thread = 1;  // consumer cells per thread of the step kernel (1 or 2)
   int dynamic_items = 1;     // work items from a device counter (1) or dealt round-robin (0)
+  int direct_pull = 0;       // the step runs the direct-pull kernel
   int occupancy = 0;
   int num_sms = 148;
   float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
@@ -216,6 +218,25 @@ int configure_step(aerosim_engine* h) {
   if (genv && atoi(genv) > 0 && atoi(genv) <= best_occ) grid = (long long)atoi(genv) * h->num_sms;
   if (grid > items) grid = items;
   h->grid = (unsigned)(grid < 1 ? 1 : grid);
+  // the direct-pull kernel (two cells per thread, no shared-memory ring; lbm_direct.cuh):
+  // AEROSIM_STEP_KERNEL=direct selects it where two cells per thread fit
+  h->direct_pull = 0;
+  if (const char* kenv = getenv("AEROSIM_STEP_KERNEL")) {
+    if (std::string(kenv) == "direct" && cpt == 2 && direct_smem_bytes(L) <= 48 * 1024) {
+      StepArgs dd = dummy;
+      dd.direct_pull = 1;
+      int occ = 0;
+      const size_t dsm = direct_smem_bytes(L);
+      CU(h, launch_step(h->cfg.precision, dd, dim3(kDirectThreads), 0, dsm, h->stream, &occ, nullptr));
+      if (occ >= 1) {
+        h->direct_pull = 1;
+        h->block = dim3(kDirectThreads);
+        h->smem = dsm;
+        h->occupancy = occ;
+        h->grid = (unsigned)(occ * h->num_sms);
+      }
+    }
+  }
   return AEROSIM_OK;
 }
 
@@ -684,6 +705,7 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.item_groups = h->item_groups;
   a.cells_per_thread = h->cells_per_thread;
   a.dynamic_items = h->dynamic_items;
+  a.direct_pull = h->direct_pull;
   a.wait_limit = h->wait_limit;
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));

@@ -4,6 +4,7 @@
 #pragma once
 #include "lbm_kernels.cuh"
 #include "lbm_batch.cuh"
+#include "lbm_direct.cuh"
 
 namespace aerosim {
 
@@ -61,6 +62,10 @@ template <class S, int MODE>
 cudaError_t step_dispatch(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s, int* occ,
                           int* launches) {
   if constexpr (MODE == MODE_FAST) {
+    if (a.direct_pull && !a.mlp_frag) {  // two cells per thread pulled from global memory (even nx)
+      if (!occ && launches) *launches = 1;
+      return direct_dispatch<S>(a, grid, smem, s, occ);  // shared memory below the 48 KB default
+    }
     if (a.mlp_frag && a.mlp_umma) {
       switch (a.L.pitch) {
         case 128: return step_entry<S, MODE, 128, MLP_TCGEN05>(a, block, grid, smem, s, occ, launches);
