@@ -15,7 +15,6 @@
 #include "engine_internal.h"
 #include "lbm_kernels.cuh"
 #include "lbm_batch.cuh"
-#include "lbm_direct.cuh"
 #include "sgs_mlp.cuh"
 
 using namespace aerosim;
@@ -43,7 +42,6 @@ struct aerosim_engine {
   int item_groups = 1;  // row groups per work item of the step kernel
   int cells_per_thread = 1;  // consumer cells per thread of the step kernel (1 or 2)
   int dynamic_items = 1;     // work items from a device counter (1) or dealt round-robin (0)
-  int direct_pull = 0;       // the step runs the direct-pull kernel
   int occupancy = 0;
   int num_sms = 148;
   float *mux = nullptr, *muy = nullptr, *muz = nullptr, *mrho = nullptr;
@@ -218,25 +216,6 @@ int configure_step(aerosim_engine* h) {
   if (genv && atoi(genv) > 0 && atoi(genv) <= best_occ) grid = (long long)atoi(genv) * h->num_sms;
   if (grid > items) grid = items;
   h->grid = (unsigned)(grid < 1 ? 1 : grid);
-  // the direct-pull kernel (two cells per thread, no shared-memory ring; lbm_direct.cuh):
-  // AEROSIM_STEP_KERNEL=direct selects it where two cells per thread fit
-  h->direct_pull = 0;
-  if (const char* kenv = getenv("AEROSIM_STEP_KERNEL")) {
-    if (std::string(kenv) == "direct" && cpt == 2 && direct_smem_bytes(L) <= 48 * 1024) {
-      StepArgs dd = dummy;
-      dd.direct_pull = 1;
-      int occ = 0;
-      const size_t dsm = direct_smem_bytes(L);
-      CU(h, launch_step(h->cfg.precision, dd, dim3(kDirectThreads), 0, dsm, h->stream, &occ, nullptr));
-      if (occ >= 1) {
-        h->direct_pull = 1;
-        h->block = dim3(kDirectThreads);
-        h->smem = dsm;
-        h->occupancy = occ;
-        h->grid = (unsigned)(occ * h->num_sms);
-      }
-    }
-  }
   return AEROSIM_OK;
 }
 
@@ -705,7 +684,6 @@ int enqueue_steps(aerosim_engine* h, int32_t n) {
   a.item_groups = h->item_groups;
   a.cells_per_thread = h->cells_per_thread;
   a.dynamic_items = h->dynamic_items;
-  a.direct_pull = h->direct_pull;
   a.wait_limit = h->wait_limit;
   long long launches = 0;
   CU(h, cudaEventRecord(h->ev0, h->stream));
@@ -1276,6 +1254,7 @@ struct aerosim_batch {
   double last_ms = 0;
   long long last_launches = 0;
   int wait_limit = kWaitLimit;  // polls of a ring wait before the batched step gives up
+  int cells_per_thread = 1;     // 2 when every instance has an even nx (pair_segment)
 };
 
 namespace {
@@ -1329,6 +1308,7 @@ BatchArgs batch_args(const aerosim_batch* b, int write_macro) {
   a.n_items = b->n_items; a.n_near = b->n_near; a.slot_elems = b->slot_elems; a.slot_cls = b->slot_cls;
   a.n_inst = (int)b->eng.size(); a.stages = b->tune.stages; a.write_macro = write_macro;
   a.wait_limit = b->wait_limit;
+  a.cells_per_thread = b->cells_per_thread;
   return a;
 }
 
@@ -1353,7 +1333,8 @@ int batch_build_items(aerosim_batch* b, int item_cells) {
     const int RY = batch_rows_per_item(L, item_cells);
     const long long rows = (long long)L.ny * L.nz;
     item_begin[k + 1] = item_begin[k] + (rows + RY - 1) / RY;
-    geo[k] = make_int4(RY, (L.nx + row_shift(L.nx) + 31) / 32, row_shift(L.nx), 0);
+    geo[k] = b->cells_per_thread == 2 ? make_int4(RY, (L.nx + 63) / 64, 0, 0)  // 64-cell pair segments
+                                      : make_int4(RY, (L.nx + row_shift(L.nx) + 31) / 32, row_shift(L.nx), 0);
     slot_elems = std::max<long long>(slot_elems, (long long)RY * 19 * L.pitch);
     slot_cls = std::max<long long>(slot_cls, (long long)RY * L.pitch);
   }
@@ -1496,6 +1477,13 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
   b->precision = prec;
   b->eng.assign(engines, engines + n);
   b->num_sms = engines[0]->num_sms;
+  // two cells per consumer thread when every instance's rows have an even cell count
+  // (AEROSIM_CELLS_PER_THREAD=1 keeps one)
+  b->cells_per_thread = 2;
+  for (int k = 0; k < n; ++k)
+    if (engines[k]->L.nx % 2 != 0 || engines[k]->L.nx < 4) b->cells_per_thread = 1;
+  if (const char* cenv = getenv("AEROSIM_CELLS_PER_THREAD"))
+    if (atoi(cenv) == 1) b->cells_per_thread = 1;
   auto bail = [&](int rc) {
     std::string msg = aerosim_last_error(nullptr);
     batch_free(b);

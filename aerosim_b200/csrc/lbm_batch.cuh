@@ -30,6 +30,7 @@ struct BatchArgs {
   long long slot_elems;          // ring slot stride (elements) and class-byte slot stride
   long long slot_cls;
   int n_inst, stages, write_macro;
+  int cells_per_thread;          // 1, or 2 when every instance has an even nx
   int wait_limit;                // polls of a ring wait before the step gives up (as StepArgs)
 };
 
@@ -49,11 +50,12 @@ __host__ __device__ inline size_t batch_smem_bytes(long long slot_elems, long lo
                                                     size_t elem) {
   return kSmemGuard + (size_t)stages * ((size_t)slot_elems * elem + (size_t)slot_cls) + kSmemGuard + 16 +
          16 * (size_t)stages + (size_t)stages * kMaxRowsPerItem * sizeof(int2) + (size_t)stages * sizeof(int) +
-         kConsumerWarps * 20 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int);
+         kConsumerWarps * 24 * sizeof(float) + 16 + 19 * sizeof(float4) + 19 * sizeof(int);
 }
 
-template <class S, int P>
-__global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
+// CPT: consumer cells per thread, 1 or 2 (pair_segment; every instance with an even nx).
+template <class S, int P, int CPT = 1>
+__global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST, MLP_NONE, CPT>())
     batch_kernel(const __grid_constant__ BatchArgs b) {
   using T = typename S::T;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -75,9 +77,9 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
   uint64_t* empty = full + S_;
   int2* s_row = reinterpret_cast<int2*>(empty + S_);            // [S_][kMaxRowsPerItem]
   int* s_inst = reinterpret_cast<int*>(s_row + S_ * kMaxRowsPerItem);  // [S_]
-  float* s_xo = reinterpret_cast<float*>(s_inst + S_);          // [kConsumerWarps][20]
+  float* s_xo = reinterpret_cast<float*>(s_inst + S_);          // [kConsumerWarps][24]
   float4* s_dcw = reinterpret_cast<float4*>(
-      (reinterpret_cast<uintptr_t>(s_xo + kConsumerWarps * 20) + 15) & ~uintptr_t(15));
+      (reinterpret_cast<uintptr_t>(s_xo + kConsumerWarps * 24) + 15) & ~uintptr_t(15));
   int* s_dslot = reinterpret_cast<int*>(s_dcw + 19);
 
   if (threadIdx.x == 0) {
@@ -235,7 +237,47 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
       long long item_sum = 0;
       int my_nan = 0;
       int ry = first / segs, sr = first - ry * segs;  // row and segment of segment `sg`
+      auto inlet = [&](int y) {
+        const double2 u = inlet_of(ia, y);
+        return make_float2((float)u.x, (float)u.y);
+      };
       for (int sg = first; sg < total; sg += kConsumerWarps) {
+        if constexpr (CPT == 2) {
+          // two adjacent cells per lane, 64-cell segments (every instance has an even nx)
+          const int cell_lo = sr * 64;
+          const int2 yz = s_row[s * kMaxRowsPerItem + ry];
+          const int iy = yz.x, iz = yz.y;
+          const T* sp = spop + (size_t)s * b.slot_elems + (size_t)ry * 19 * pitch;
+          const uint8_t* sc = scls + (size_t)s * b.slot_cls + (size_t)ry * pitch;
+          const int x0 = cell_lo + 2 * lane;
+          const bool active = x0 < nx;
+          const int lx = active ? x0 : 0;  // lanes outside the row read cells 0 and 1
+          const uint32_t cls2 = *reinterpret_cast<const uint16_t*>(sc + lx);
+          float2 v[19];
+#pragma unroll
+          for (int d = 0; d < 19; ++d) {
+            const T* q = sp + slot_of(d) * pitch + lx;
+            if (cx_of(d) == 0) v[d] = load_pair<S>(q);
+            else v[d] = make_float2(S::raw(q[-cx_of(d)]), S::raw(q[1 - cx_of(d)]));
+          }
+          if (sg + kConsumerWarps >= total) {  // this warp's last segment of the slot
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+          }
+          PairGeom g;
+          g.row = row0 + ry; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
+          g.iy = iy; g.iz = iz; g.x0 = x0; g.cell_lo = cell_lo; g.active = active;
+          g.has_lo = cell_lo == 0;
+          g.has_hi = cell_lo <= nx - 2 && nx - 2 < cell_lo + 64;
+          g.wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
+          g.ground_no_slip = ia.ground_no_slip; g.write_macro = b.write_macro;
+          g.c0 = (uint8_t)(cls2 & 0xffu);
+          g.c1 = (uint8_t)(cls2 >> 8);
+          pair_segment<S>(v, fd, g, tau0f, ksmagf, dec, inlet, ia, s_xo + warp * 24, s_dcw, s_dslot, lane,
+                          item_sum, my_nan);
+          for (sr += kConsumerWarps; sr >= segs; sr -= segs) ++ry;
+          continue;
+        }
         const int cell_lo = sr * 32 - shift;
         const int2 yz = s_row[s * kMaxRowsPerItem + ry];
         const int iy = yz.x, iz = yz.y;
@@ -258,12 +300,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST>())
         g.row_ok = true; g.active = active; g.near = (cl & CLS_NEAR) != 0;
         g.wall_row = (iy == 0 || iy == ny - 1 || (nz > 4 && (iz == 0 || iz == nz - 1)));
         g.ground_no_slip = ia.ground_no_slip; g.write_macro = b.write_macro; g.cl = cl;
-        fast_segment<S>(v, fd, g, tau0f, ksmagf, dec,
-                        [&](int y) {
-                          const double2 u = inlet_of(ia, y);
-                          return make_float2((float)u.x, (float)u.y);
-                        },
-                        ia, s_xo + warp * 20, s_dcw, s_dslot, lane, item_sum, my_nan);
+        fast_segment<S>(v, fd, g, tau0f, ksmagf, dec, inlet, ia, s_xo + warp * 24, s_dcw, s_dslot, lane, item_sum,
+                        my_nan);
         for (sr += kConsumerWarps; sr >= segs; sr -= segs) ++ry;
       }
 #pragma unroll

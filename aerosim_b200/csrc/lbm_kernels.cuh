@@ -89,7 +89,6 @@ struct StepArgs {
   int wait_limit;         // polls of a ring wait before the step gives up (kWaitLimit;
                           //   0 gives up at once: the failure path's test)
   int cells_per_thread;   // consumer cells per thread: 1, or 2 (pair kernels, even nx)
-  int direct_pull;        // 1: the direct-pull kernel (lbm_direct.cuh) runs the step
   int dynamic_items;      // 1: CTAs take work items from a device counter (StepState::next_item)
                           //   instead of the static round-robin deal
 };

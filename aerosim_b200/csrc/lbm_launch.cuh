@@ -4,7 +4,6 @@
 #pragma once
 #include "lbm_kernels.cuh"
 #include "lbm_batch.cuh"
-#include "lbm_direct.cuh"
 
 namespace aerosim {
 
@@ -62,10 +61,6 @@ template <class S, int MODE>
 cudaError_t step_dispatch(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s, int* occ,
                           int* launches) {
   if constexpr (MODE == MODE_FAST) {
-    if (a.direct_pull && !a.mlp_frag) {  // two cells per thread pulled from global memory (even nx)
-      if (!occ && launches) *launches = 1;
-      return direct_dispatch<S>(a, grid, smem, s, occ);  // shared memory below the 48 KB default
-    }
     if (a.mlp_frag && a.mlp_umma) {
       switch (a.L.pitch) {
         case 128: return step_entry<S, MODE, 128, MLP_TCGEN05>(a, block, grid, smem, s, occ, launches);
@@ -108,11 +103,11 @@ cudaError_t step_dispatch(const StepArgs& a, dim3 block, unsigned grid, size_t s
   return step_entry<S, MODE, 0>(a, block, grid, smem, s, occ, launches);
 }
 
-// One step of a batch (batch_kernel).  pitch: the row pitch shared by every instance,
-// or 0 when the instances differ (the kernel then reads each instance's pitch).
-template <class S, int P>
+// One step of a batch (batch_kernel) for a row pitch P (0: run time) and CPT cells per
+// consumer thread.
+template <class S, int P, int CPT>
 cudaError_t batch_entry(const BatchArgs& b, unsigned grid, size_t smem, cudaStream_t s, int* occ) {
-  auto k = batch_kernel<S, P>;
+  auto k = batch_kernel<S, P, CPT>;
   if (occ) {
     cudaError_t e = raise_smem_limit(k);
     if (e != cudaSuccess) return e;
@@ -122,15 +117,23 @@ cudaError_t batch_entry(const BatchArgs& b, unsigned grid, size_t smem, cudaStre
   return cudaGetLastError();
 }
 
+template <class S, int CPT>
+cudaError_t batch_dispatch_cpt(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s, int* occ) {
+  switch (pitch) {
+    case 64: return batch_entry<S, 64, CPT>(b, grid, smem, s, occ);
+    case 128: return batch_entry<S, 128, CPT>(b, grid, smem, s, occ);
+    case 192: return batch_entry<S, 192, CPT>(b, grid, smem, s, occ);
+    case 256: return batch_entry<S, 256, CPT>(b, grid, smem, s, occ);
+    default: return batch_entry<S, 0, CPT>(b, grid, smem, s, occ);
+  }
+}
+
+// One step of a batch (batch_kernel).  pitch: the row pitch shared by every instance,
+// or 0 when the instances differ (the kernel then reads each instance's pitch).
 template <class S>
 cudaError_t batch_dispatch(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s, int* occ) {
-  switch (pitch) {
-    case 64: return batch_entry<S, 64>(b, grid, smem, s, occ);
-    case 128: return batch_entry<S, 128>(b, grid, smem, s, occ);
-    case 192: return batch_entry<S, 192>(b, grid, smem, s, occ);
-    case 256: return batch_entry<S, 256>(b, grid, smem, s, occ);
-    default: return batch_entry<S, 0>(b, grid, smem, s, occ);
-  }
+  return b.cells_per_thread == 2 ? batch_dispatch_cpt<S, 2>(b, pitch, grid, smem, s, occ)
+                                 : batch_dispatch_cpt<S, 1>(b, pitch, grid, smem, s, occ);
 }
 
 }  // namespace aerosim

@@ -116,6 +116,25 @@ def test_fp16_engines_alone_match_a_batch_across_widths(oracle_mod, monkeypatch)
         ea.close()
 
 
+@pytest.mark.parametrize("precision", ["f16s", "bf16s"])
+def test_batch_two_cells_per_thread_matches_engines_alone(oracle_mod, precision):
+    """Instances whose rows all have an even cell count run two cells per consumer thread
+    in the batched kernel, like the engines stepped alone: the same pair arithmetic, so
+    within a storage rounding of each other."""
+    dims = [(64, 24, 24), (96, 32, 24), (160, 24, 32)]
+    cs = [_case(nx, ny, nz, 3.0 + k, nx / 3) for k, (nx, ny, nz) in enumerate(dims)]
+    pairs = [(_engine(oracle_mod, c, precision), _engine(oracle_mod, c, precision)) for c in cs]
+    batch = LBMBatch([p[0][1] for p in pairs])
+    batch.step(50)
+    for (vox, eb), (_, ea) in pairs:
+        ea.step(50)
+        _compare(eb, ea, vox, 1e-5, atol=1e-5 if precision == "f16s" else 1e-4)
+    batch.close()
+    for (_, eb), (_, ea) in pairs:
+        eb.close()
+        ea.close()
+
+
 def test_batch_graph_replay_equals_single_launches(oracle_mod):
     """graph_steps = 5 over 12 steps (two replays and two single launches) against
     graph_steps = 1 (every step its own launch), FP16 storage."""
