@@ -55,10 +55,9 @@ def _peaks():
 
 
 def _profile_traffic(precision: str):
-    """DRAM bytes per step-kernel launch from the committed ncu summary, if any (the 16-bit
-    storage kernels run with 4-row work items)."""
+    """DRAM bytes per step-kernel launch from the committed ncu summary, if any."""
     name = ("main_kernel_ellipsoid_256x128x128.md" if precision == "f32"
-            else "main_kernel_f16s_4row_items_ellipsoid_256x128x128.md")
+            else "main_kernel_f16s_pairs_ellipsoid_256x128x128.md")
     path = os.path.join(ROOT, "profiles", name)
     try:
         text = open(path).read()
