@@ -145,7 +145,7 @@ SIGNATURES = {
     "aerosim_set_sgs_mlp": ([_P, _F32P], C.c_int),
     "aerosim_set_sgs_mlp_path": ([_P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "aerosim_read_wall_distance": ([_P, _F32P], C.c_int),
-    "aerosim_sgs_samples": ([_P, _P, C.c_float, C.c_int32, _F32P, _F32P, _U8P], C.c_int),
+    "aerosim_sgs_samples": ([_P, _P, C.c_float, C.c_float, C.c_int32, _F32P, _F32P, _U8P], C.c_int),
     "aerosim_frontal_area": ([_F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P], C.c_int),
     "aerosim_frontal_area_cuda": ([C.c_int32, _F32P, C.c_int64, _I32P, C.c_int64, _F64P, C.c_int32, _F64P],
                                   C.c_int),

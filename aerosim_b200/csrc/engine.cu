@@ -1186,9 +1186,10 @@ int aerosim_read_wall_distance(aerosim_engine* h, float* out) {
   return AEROSIM_OK;
 }
 
-int aerosim_sgs_samples(aerosim_engine* fine, aerosim_engine* coarse, float max_ratio, int32_t average_radius,
-                        float* X, float* Y, uint8_t* valid) {
-  if (!fine || !coarse || !X || !Y || !valid || !(max_ratio > 0.0f) || average_radius < 0 || average_radius > 4)
+int aerosim_sgs_samples(aerosim_engine* fine, aerosim_engine* coarse, float min_ratio, float max_ratio,
+                        int32_t average_radius, float* X, float* Y, uint8_t* valid) {
+  if (!fine || !coarse || !X || !Y || !valid || !(max_ratio > 0.0f) || !(min_ratio <= 0.0f) ||
+      !(min_ratio >= -max_ratio) || average_radius < 0 || average_radius > 4)
     return fail(nullptr, AEROSIM_ERR_ARG, "sgs_samples: bad argument");
   if (!fine->have_grid || !fine->f[0] || !coarse->have_grid)
     return fail(nullptr, AEROSIM_ERR_STATE, "sgs_samples: both engines need a voxel grid (and the fine one a flow)");
@@ -1208,7 +1209,8 @@ int aerosim_sgs_samples(aerosim_engine* fine, aerosim_engine* coarse, float max_
   if (e == cudaSuccess) e = cudaMalloc(&dv, Nc);
   if (e == cudaSuccess)
     e = launch_sgs_samples(fine->mux, fine->muy, fine->muz, fine->mrho, f.flags, f.nx, f.ny, f.nz, c.cls,
-                           coarse->L.pitch, c.nx, c.ny, c.nz, (float)effective_nu0(coarse), max_ratio, average_radius,
+                           coarse->L.pitch, c.nx, c.ny, c.nz, (float)effective_nu0(coarse), min_ratio, max_ratio,
+                           average_radius,
                            dx, dy, dv,
                            coarse->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(X, dx, Nc * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, coarse->stream);

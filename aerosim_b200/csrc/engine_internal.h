@@ -83,7 +83,7 @@ cudaError_t compute_wall_distance(const uint8_t* flags, int nx, int ny, int nz, 
                                   cudaStream_t s);
 cudaError_t launch_sgs_samples(const float* ux, const float* uy, const float* uz, const float* rho,
                                const uint8_t* fflags, int fx, int fy, int fz, const uint8_t* ccls, int cpitch, int cx,
-                               int cy, int cz, float nu0, float max_ratio, int avg, float* X, float* Y,
-                               uint8_t* valid, cudaStream_t s);
+                               int cy, int cz, float nu0, float min_ratio, float max_ratio, int avg, float* X,
+                               float* Y, uint8_t* valid, cudaStream_t s);
 
 }  // namespace aerosim

@@ -404,10 +404,13 @@ __global__ void sgs_sample_kernel(const float* __restrict__ ubar, const float* _
 
 // Pass 3: the target nu_t / nu_0 of a valid cell: numerators and denominators summed
 // over the valid cells of its (2 avg + 1)^3 neighbourhood, then divided and clipped to
-// [0, max_ratio] (least-squares averaging, which keeps the sign information that a
-// per-cell clip at zero would discard).
+// [min_ratio, max_ratio] (least-squares averaging, which keeps the sign information that a
+// per-cell clip at zero would discard; min_ratio < 0 keeps backscatter in the targets, so
+// that a regression onto a non-negative output learns the conditional mean rather than
+// the mean of the clipped values, which lies above it).
 __global__ void sgs_target_kernel(const float2* __restrict__ nd, const uint8_t* __restrict__ valid, int cx, int cy,
-                                  int cz, int avg, float nu0, float max_ratio, float* __restrict__ Yo) {
+                                  int cz, int avg, float nu0, float min_ratio, float max_ratio,
+                                  float* __restrict__ Yo) {
   const long long Nc = (long long)cx * cy * cz;
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < Nc; c += (long long)gridDim.x * blockDim.x) {
     if (!valid[c]) {
@@ -428,7 +431,7 @@ __global__ void sgs_target_kernel(const float2* __restrict__ nd, const uint8_t* 
           d += v.y;
         }
     float nut = d > 0.0f ? n / d : 0.0f;
-    nut = fminf(fmaxf(nut, 0.0f), max_ratio * nu0);
+    nut = fminf(fmaxf(nut, min_ratio * nu0), max_ratio * nu0);
     Yo[c] = nut / nu0;
   }
 }
@@ -509,8 +512,8 @@ cudaError_t compute_wall_distance(const uint8_t* flags, int nx, int ny, int nz, 
 
 cudaError_t launch_sgs_samples(const float* ux, const float* uy, const float* uz, const float* rho,
                                const uint8_t* fflags, int fx, int fy, int fz, const uint8_t* ccls, int cpitch, int cx,
-                               int cy, int cz, float nu0, float max_ratio, int avg, float* X, float* Y,
-                               uint8_t* valid, cudaStream_t s) {
+                               int cy, int cz, float nu0, float min_ratio, float max_ratio, int avg, float* X,
+                               float* Y, uint8_t* valid, cudaStream_t s) {
   const long long Nc = (long long)cx * cy * cz;
   float *ubar = nullptr, *uu = nullptr;
   float2* nd = nullptr;
@@ -521,7 +524,7 @@ cudaError_t launch_sgs_samples(const float* ux, const float* uy, const float* uz
   if (e == cudaSuccess) {
     sgs_filter_kernel<<<grid, 256, 0, s>>>(ux, uy, uz, rho, fflags, fx, fy, fz, cx, cy, cz, ubar, uu);
     sgs_sample_kernel<<<grid, 256, 0, s>>>(ubar, uu, ccls, cpitch, cx, cy, cz, X, nd, valid);
-    sgs_target_kernel<<<grid, 256, 0, s>>>(nd, valid, cx, cy, cz, avg, nu0, max_ratio, Y);
+    sgs_target_kernel<<<grid, 256, 0, s>>>(nd, valid, cx, cy, cz, avg, nu0, min_ratio, max_ratio, Y);
     e = cudaGetLastError();
   }
   cudaFreeAsync(ubar, s);

@@ -81,15 +81,17 @@ def train(params, X, Y, iters: int = 2000, batch: int = 8192, lr: float = 2e-3, 
     return p, curve
 
 
-def samples(fine, coarse, max_ratio: float = 50.0, average_radius: int = 0):
+def samples(fine, coarse, max_ratio: float = 50.0, average_radius: int = 0, min_ratio: float = 0.0):
     """(X, Y) of the valid coarse cells from the flow of engine `fine` box-filtered onto
     engine `coarse` (a lattice exactly half as fine); the eddy-viscosity target is the
-    least-squares fit over each cell's (2 average_radius + 1)^3 neighbourhood."""
+    least-squares fit over each cell's (2 average_radius + 1)^3 neighbourhood, clipped to
+    [min_ratio, max_ratio] x nu_0 (a negative min_ratio keeps backscatter)."""
     n = coarse.voxel_info().nx * coarse.voxel_info().ny * coarse.voxel_info().nz
     X = np.empty((n, N_IN), np.float32)
     Y = np.empty(n, np.float32)
     V = np.empty(n, np.uint8)
-    N.check(N.load().aerosim_sgs_samples(fine._h.h, coarse._h.h, float(max_ratio), int(average_radius),
+    N.check(N.load().aerosim_sgs_samples(fine._h.h, coarse._h.h, float(min_ratio), float(max_ratio),
+                                         int(average_radius),
                                          N.ptr(X, C.c_float),
                                          N.ptr(Y, C.c_float), N.ptr(V, C.c_uint8)))
     ok = V != 0

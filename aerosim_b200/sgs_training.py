@@ -9,13 +9,15 @@
    box-filtered onto the
    256x128x128 lattice into training samples (aerosim_sgs_samples).
    The eddy-viscosity target is the least-squares fit of the subgrid stress per coarse
-   cell, clipped at zero, or over each cell's (2r+1)^3 neighbourhood (--average-radius r).
+   cell, or over each cell's (2r+1)^3 neighbourhood (--average-radius r), clipped below at
+   --min-ratio x nu_0 (0: no backscatter; a negative bound keeps it in the targets).
 2. Training on the GPU (aerosim_mlp_train, Adam) on all snapshots but the last; the
    last one is held out: the closure's eddy viscosity and Smagorinsky's are both scored
    against the filtered subgrid stress (mean squared error of nu_t / nu_0).
 3. Coarse runs at 256x128x128 over the same physical time (half the steps): plain
    Smagorinsky and the learned closure.  Cd over the second half of each run against the
-   fine run's, and device time of each run.
+   fine run's (with the standard error of each mean from 10 block means), and device time
+   of each run.
 
 The weights are written to `--weights` (FP32 parameter vector, aerosim_b200.sgs
 layout) and the metrics to `--out`.
@@ -59,6 +61,16 @@ def _run(e: LBMEngine, steps: int, every: int, on_sample=None):
     return np.array(cd), ms
 
 
+def block_se(x: np.ndarray, blocks: int = 10) -> float:
+    """Standard error of the mean of a correlated series from the means of `blocks`
+    consecutive blocks (batch means); 0 for fewer samples than blocks."""
+    n = (len(x) // blocks) * blocks
+    if n < blocks or blocks < 2:
+        return 0.0
+    m = x[:n].reshape(blocks, -1).mean(axis=1)
+    return float(m.std(ddof=1) / np.sqrt(blocks))
+
+
 def main(argv=None) -> dict:
     ap = argparse.ArgumentParser()
     ap.add_argument("--fine-steps", type=int, default=24000)
@@ -70,6 +82,8 @@ def main(argv=None) -> dict:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--average-radius", type=int, default=0,
                     help="least-squares eddy viscosity over (2r+1)^3 coarse cells (0: per cell)")
+    ap.add_argument("--min-ratio", type=float, default=0.0,
+                    help="lower clip of the targets in units of nu_0 (negative: keep backscatter)")
     ap.add_argument("--scale", type=int, default=1, help="1: 512x256x256 / 256x128x128; 2: half of each")
     ap.add_argument("--out", default="")
     ap.add_argument("--weights", default="")
@@ -78,7 +92,8 @@ def main(argv=None) -> dict:
     nx, ny, nz = 256 // a.scale, 128 // a.scale, 128 // a.scale
     fine_case = cases.scaled_ellipsoid(2 * nx, 2 * ny, 2 * nz)
     coarse_case = cases.scaled_ellipsoid(nx, ny, nz)
-    res: dict = {"fine": f"{2 * nx}x{2 * ny}x{2 * nz}", "coarse": f"{nx}x{ny}x{nz}", "fine_steps": a.fine_steps}
+    res: dict = {"fine": f"{2 * nx}x{2 * ny}x{2 * nz}", "coarse": f"{nx}x{ny}x{nz}", "fine_steps": a.fine_steps,
+                 "min_ratio": a.min_ratio, "average_radius": a.average_radius}
 
     # ---- 1. fine plain run and training samples ----
     t0 = time.perf_counter()
@@ -88,7 +103,7 @@ def main(argv=None) -> dict:
 
     def take(step):
         if step > a.fine_steps // 2 and step % a.snapshot_every == 0:
-            X, Y = sgs.samples(fine, coarse_geo, average_radius=a.average_radius)
+            X, Y = sgs.samples(fine, coarse_geo, average_radius=a.average_radius, min_ratio=a.min_ratio)
             k = min(a.samples_per_snapshot, X.shape[0])
             sel = rng.choice(X.shape[0], k, replace=False)
             snaps.append((X[sel], Y[sel]))
@@ -96,6 +111,7 @@ def main(argv=None) -> dict:
     cd_f, ms_f = _run(fine, a.fine_steps, 200, take)
     res["fine_cd_mean"] = float(cd_f.mean())
     res["fine_cd_std"] = float(cd_f.std())
+    res["fine_cd_se"] = block_se(cd_f)
     res["fine_device_ms"] = ms_f
     res["snapshots"] = len(snaps)
     fine.close()
@@ -125,8 +141,11 @@ def main(argv=None) -> dict:
             e.set_sgs_mlp(params)
         cd, ms = _run(e, steps_c, 100)
         m = e.mass_stats()
-        res[name] = {"cd_mean": float(cd.mean()), "cd_std": float(cd.std()), "device_ms": ms,
+        se = block_se(cd)
+        res[name] = {"cd_mean": float(cd.mean()), "cd_std": float(cd.std()), "cd_se": se, "device_ms": ms,
                      "cd_err_vs_fine": float(abs(cd.mean() - res["fine_cd_mean"]) / abs(res["fine_cd_mean"])),
+                     # standard error of the relative difference (both means' block errors)
+                     "cd_err_se": float(np.hypot(se, res["fine_cd_se"]) / abs(res["fine_cd_mean"])),
                      "speedup_vs_fine": ms_f / ms, "nan": bool(m["hasNaN"])}
         e.close()
     res["wall_s"] = time.perf_counter() - t0

@@ -283,10 +283,11 @@ int aerosim_read_wall_distance(aerosim_engine* h, float* out);
  * step) box-filtered onto `coarse`, whose lattice is exactly half as fine: per coarse
  * cell X[8] (filtered strain rate, density, wall distance as the closure sees them),
  * Y = nu_t / nu_0 of the least-squares eddy viscosity of the subgrid stress over the
- * (2 average_radius + 1)^3 neighbourhood (0..4), clipped to [0, max_ratio], and valid
+ * (2 average_radius + 1)^3 neighbourhood (0..4), clipped to [min_ratio, max_ratio]
+ * (-max_ratio <= min_ratio <= 0; 0 drops backscatter, a negative bound keeps it), and valid
  * (0 at solid, boundary-adjacent and edge cells). */
-int aerosim_sgs_samples(aerosim_engine* fine, aerosim_engine* coarse, float max_ratio, int32_t average_radius,
-                        float* X, float* Y, uint8_t* valid);
+int aerosim_sgs_samples(aerosim_engine* fine, aerosim_engine* coarse, float min_ratio, float max_ratio,
+                        int32_t average_radius, float* X, float* Y, uint8_t* valid);
 
 /* ---- batches: many tunnels in one launch --------------------------------- */
 
