@@ -204,6 +204,7 @@ __global__ void slice_kernel(const float* __restrict__ mux, const float* __restr
                              const uint8_t* __restrict__ cls, const StepState* st, int prev_slot, const Layout L,
                              int axis, int fixed, int mode, double uref, int width, int height,
                              uint8_t* __restrict__ rgba) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // programmatic dependent of the frame's kernels
   const int apply = prev_slot >= 0 ? st->apply[prev_slot] : 0;
   const double corr = apply ? st->corr[prev_slot] : 1.0;
   const int nx = L.nx, ny = L.ny, nz = L.nz;

@@ -32,16 +32,33 @@ cudaError_t launch_step(int precision, const StepArgs& a, dim3 block, unsigned g
   }
 }
 
+// A launch as a programmatic dependent of the kernel before it on the stream: its CTAs may
+// be scheduled while that kernel finishes and wait (griddepcontrol.wait) for its completion.
+template <class K, class... Args>
+static cudaError_t launch_dependent(K kernel, unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 cudaError_t launch_forces(int precision, const ForceArgs& a, unsigned grid, cudaStream_t s) {
   switch (precision) {
-    case AEROSIM_PREC_F32: forces_kernel<StoreF32S, MODE_FAST><<<grid, 256, 0, s>>>(a); break;
-    case AEROSIM_PREC_F32_MIRROR: forces_kernel<StoreF32, MODE_MIRROR><<<grid, 256, 0, s>>>(a); break;
-    case AEROSIM_PREC_F16S: forces_kernel<StoreF16S, MODE_FAST><<<grid, 256, 0, s>>>(a); break;
-    case AEROSIM_PREC_BF16S: forces_kernel<StoreBF16S, MODE_FAST><<<grid, 256, 0, s>>>(a); break;
-    case AEROSIM_PREC_F64: forces_kernel<StoreF64, MODE_F64><<<grid, 256, 0, s>>>(a); break;
+    case AEROSIM_PREC_F32: return launch_dependent(forces_kernel<StoreF32S, MODE_FAST>, grid, 256, s, a);
+    case AEROSIM_PREC_F32_MIRROR: return launch_dependent(forces_kernel<StoreF32, MODE_MIRROR>, grid, 256, s, a);
+    case AEROSIM_PREC_F16S: return launch_dependent(forces_kernel<StoreF16S, MODE_FAST>, grid, 256, s, a);
+    case AEROSIM_PREC_BF16S: return launch_dependent(forces_kernel<StoreBF16S, MODE_FAST>, grid, 256, s, a);
+    case AEROSIM_PREC_F64: return launch_dependent(forces_kernel<StoreF64, MODE_F64>, grid, 256, s, a);
     default: return cudaErrorInvalidValue;
   }
-  return cudaGetLastError();
 }
 
 static unsigned grid_for(long long n) {
@@ -147,9 +164,8 @@ cudaError_t launch_slice(const float* mux, const float* muy, const float* muz, c
                          int mode, double uref, int width, int height, uint8_t* rgba, cudaStream_t s) {
   const long long P = (long long)width * height;
   const int grid = (int)std::min<long long>((P + 255) / 256, 1184);
-  slice_kernel<<<grid, 256, 0, s>>>(mux, muy, muz, mrho, cls, st, prev_slot, L, axis, fixed, mode, uref, width,
-                                    height, rgba);
-  return cudaGetLastError();
+  return launch_dependent(slice_kernel, (unsigned)grid, 256, s, mux, muy, muz, mrho, cls, st, prev_slot, L, axis,
+                          fixed, mode, uref, width, height, rgba);
 }
 
 cudaError_t launch_q_criterion(int nx, int ny, int nz, double dx, const float* ux, const float* uy, const float* uz,

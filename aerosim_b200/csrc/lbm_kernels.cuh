@@ -1552,6 +1552,11 @@ __global__ void __launch_bounds__(256) forces_kernel(const ForceArgs a) {
   using T = typename S::T;
   __shared__ double red[8][8];
   __shared__ bool is_last;
+  // launched as a programmatic dependent of the step kernel in a frame: wait for the step
+  // to complete before reading its populations (a no-op after an ordinary launch), and let
+  // the slice kernel that follows start its launch
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const T* __restrict__ f = static_cast<const T*>(a.f);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int apply = a.prev_slot >= 0 ? a.st->apply[a.prev_slot] : 0;
