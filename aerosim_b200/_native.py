@@ -21,11 +21,12 @@ STL_BINARY, STL_ASCII = 0, 1
 
 CELL_FLUID, CELL_SOLID, CELL_BOUNDARY = 0, 1, 2
 
-PREC_F32, PREC_F32_MIRROR, PREC_F16S, PREC_BF16S, PREC_F64 = 0, 1, 2, 3, 4
+PREC_F32, PREC_F32_MIRROR, PREC_F16S, PREC_BF16S, PREC_F64, PREC_F16C = 0, 1, 2, 3, 4, 5
 PRECISIONS = {"f32": PREC_F32, "f32_mirror": PREC_F32_MIRROR, "f16s": PREC_F16S,
-              "bf16s": PREC_BF16S, "f64": PREC_F64}
+              "bf16s": PREC_BF16S, "f64": PREC_F64, "f16c": PREC_F16C}
 # bytes of population storage per cell and step (19 reads + 19 writes)
-BYTES_PER_CELL = {PREC_F32: 152, PREC_F32_MIRROR: 152, PREC_F16S: 76, PREC_BF16S: 76, PREC_F64: 304}
+BYTES_PER_CELL = {PREC_F32: 152, PREC_F32_MIRROR: 152, PREC_F16S: 76, PREC_BF16S: 76, PREC_F64: 304,
+                  PREC_F16C: 76}
 
 DTYPE_F32, DTYPE_F64 = 0, 1
 

@@ -36,6 +36,7 @@ UNITS = {
     "lbm_fast_f32.cu": [],
     "lbm_fast_f16s.cu": [],
     "lbm_fast_bf16s.cu": [],
+    "lbm_fast_f16c.cu": [],
     "lbm_exact.cu": ["-fmad=false"],
     "voxelize.cu": ["-fmad=false"],
     "engine.cu": [],

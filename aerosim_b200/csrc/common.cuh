@@ -51,7 +51,7 @@ __host__ __device__ inline double js_max(double a, double b) {
 constexpr float F16S_SCALE = 32768.0f;
 constexpr float F16S_INV_SCALE = 1.0f / 32768.0f;
 
-// Population storage codecs.  All five expose the same interface in terms of the
+// Population storage codecs.  All six expose the same interface in terms of the
 // deviation h = f - w_d from the rest weight (the form the FP32 collision works in)
 // and of the full value f (the form the FP64 paths work in):
 //   h_of(raw, d), raw_of_h(h, d)  -- float deviation
@@ -66,6 +66,7 @@ struct StoreF32 {
   using T = float;
   // FP32-collision output in the storage domain: value = kOutScale * h + kOutW * w_d
   static constexpr float kOutScale = 1.0f, kOutW = 1.0f;
+  static constexpr bool kCompensate = false;
   static constexpr bool kRawMoments = false;
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return v; }
@@ -82,6 +83,7 @@ struct StoreF32 {
 struct StoreF32S {
   using T = float;
   static constexpr float kOutScale = 1.0f, kOutW = 0.0f;
+  static constexpr bool kCompensate = false;
   static constexpr bool kRawMoments = true;
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return v; }
@@ -94,6 +96,7 @@ struct StoreF32S {
 struct StoreF64 {
   using T = double;
   static constexpr float kOutScale = 1.0f, kOutW = 1.0f;
+  static constexpr bool kCompensate = false;
   static constexpr bool kRawMoments = false;
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return (float)v; }
@@ -106,6 +109,7 @@ struct StoreF64 {
 struct StoreF16S {
   using T = __half;
   static constexpr float kOutScale = F16S_SCALE, kOutW = 0.0f;
+  static constexpr bool kCompensate = false;
   static constexpr bool kRawMoments = true;
   static constexpr float kRawScale = F16S_INV_SCALE;
   __device__ __forceinline__ static float raw(T v) { return __half2float(v); }
@@ -118,6 +122,7 @@ struct StoreF16S {
 struct StoreBF16S {
   using T = __nv_bfloat16;
   static constexpr float kOutScale = 1.0f, kOutW = 0.0f;
+  static constexpr bool kCompensate = false;
   static constexpr bool kRawMoments = true;
   static constexpr float kRawScale = 1.0f;
   __device__ __forceinline__ static float raw(T v) { return __bfloat162float(v); }
@@ -127,6 +132,44 @@ struct StoreBF16S {
   __device__ __forceinline__ static double f_of(T v, int d) { return (double)wf_of(d) + (double)h_of(v, d); }
   __device__ __forceinline__ static T raw_of_f(double f, int d) { return raw_of_h((float)(f - (double)wf_of(d)), d); }
 };
+// FP16 shifted storage with mass-compensated rounding: the values are those of StoreF16S,
+// but wherever a step kernel stores a cell it rounds the 18 moving populations first and
+// gives the rest population what their rounded values leave of the cell's deviation sum
+// (compensate_cell and its lane form below, and the pair path of pair_segment), i.e. the
+// rest population absorbs their rounding errors before it rounds itself.  The stored
+// deviations of a cell then sum to the computed ones up to the single rounding of f_0,
+// whose half-precision ulp is 4-8 times finer than the moving populations' near
+// equilibrium (|f_0 - w_0| is of the order of 1.5 w_0 u^2, |f_d - w_d| of 3 w_d |c_d . u|),
+// where the uncompensated error grows like the square root of 18 roundings.  Initial,
+// written and rescaled fields round per value, like StoreF16S.
+struct StoreF16C : StoreF16S {
+  static constexpr bool kCompensate = true;
+};
+
+// Mass-compensated rounding of one cell's 19 values v (storage domain, direction order):
+// the rounding errors of directions 1..18 move into direction 0.  No-op for the codecs
+// without kCompensate.
+template <class S>
+__device__ __forceinline__ void compensate_cell(float (&v)[19]) {
+  if constexpr (S::kCompensate) {
+    float e = 0.0f;
+#pragma unroll
+    for (int d = 1; d < 19; ++d) e += v[d] - S::raw(S::store(v[d]));
+    v[0] += e;
+  }
+}
+// The same for a cell written lane-transposed (lane d < 19 holds direction d); every lane
+// of the warp calls it.
+template <class S>
+__device__ __forceinline__ float compensate_lanes(float v, int lane) {
+  if constexpr (S::kCompensate) {
+    float e = (lane >= 1 && lane < 19) ? v - S::raw(S::store(v)) : 0.0f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if (lane == 0) v += e;
+  }
+  return v;
+}
 
 // Storage order of the directions inside a row block ("slots"): directions that pull
 // from the same source row (same c_y, c_z) are adjacent, so one bulk copy brings all

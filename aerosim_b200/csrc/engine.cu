@@ -160,7 +160,8 @@ int configure_step(aerosim_engine* h) {
   dummy.mlp_frag = h->mlp_frag;
   dummy.mlp_umma = closure_umma(h);
   const int mlp = h->mlp_frag ? (dummy.mlp_umma ? 2 : 1) : 0;
-  const bool half = h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S;
+  const bool half = h->cfg.precision == AEROSIM_PREC_F16S || h->cfg.precision == AEROSIM_PREC_BF16S ||
+                    h->cfg.precision == AEROSIM_PREC_F16C;
   const bool fast = half || h->cfg.precision == AEROSIM_PREC_F32;
   // two cells per consumer thread (packed FP32 pairs) without the closure on rows of an
   // even cell count; AEROSIM_CELLS_PER_THREAD (1 or 2) overrides the choice for any
@@ -1471,8 +1472,8 @@ int aerosim_batch_create(aerosim_engine* const* engines, int32_t n, aerosim_batc
       if (engines[j] == e) return bfail(AEROSIM_ERR_ARG, "batch_create: an engine appears twice");
   }
   const int prec = engines[0]->cfg.precision;
-  if (prec != AEROSIM_PREC_F32 && prec != AEROSIM_PREC_F16S && prec != AEROSIM_PREC_BF16S)
-    return bfail(AEROSIM_ERR_ARG, "batch_create: batches run the F32, F16S and BF16S precisions");
+  if (prec != AEROSIM_PREC_F32 && prec != AEROSIM_PREC_F16S && prec != AEROSIM_PREC_BF16S && prec != AEROSIM_PREC_F16C)
+    return bfail(AEROSIM_ERR_ARG, "batch_create: batches run the F32, F16S, BF16S and F16C precisions");
   aerosim_batch* b = new (std::nothrow) aerosim_batch();
   if (!b) return bfail(AEROSIM_ERR_NOMEM, "batch_create: out of host memory");
   b->device = engines[0]->device;

@@ -17,7 +17,7 @@ cudaError_t launch_step_fast(int precision, const StepArgs& a, dim3 block, unsig
 size_t precision_bytes(int precision) {
   switch (precision) {
     case AEROSIM_PREC_F32: case AEROSIM_PREC_F32_MIRROR: return 4;
-    case AEROSIM_PREC_F16S: case AEROSIM_PREC_BF16S: return 2;
+    case AEROSIM_PREC_F16S: case AEROSIM_PREC_BF16S: case AEROSIM_PREC_F16C: return 2;
     case AEROSIM_PREC_F64: return 8;
     default: return 0;
   }
@@ -54,7 +54,7 @@ cudaError_t launch_forces(int precision, const ForceArgs& a, unsigned grid, cuda
   switch (precision) {
     case AEROSIM_PREC_F32: return launch_dependent(forces_kernel<StoreF32S, MODE_FAST>, grid, 256, s, a);
     case AEROSIM_PREC_F32_MIRROR: return launch_dependent(forces_kernel<StoreF32, MODE_MIRROR>, grid, 256, s, a);
-    case AEROSIM_PREC_F16S: return launch_dependent(forces_kernel<StoreF16S, MODE_FAST>, grid, 256, s, a);
+    case AEROSIM_PREC_F16S: case AEROSIM_PREC_F16C: return launch_dependent(forces_kernel<StoreF16S, MODE_FAST>, grid, 256, s, a);
     case AEROSIM_PREC_BF16S: return launch_dependent(forces_kernel<StoreBF16S, MODE_FAST>, grid, 256, s, a);
     case AEROSIM_PREC_F64: return launch_dependent(forces_kernel<StoreF64, MODE_F64>, grid, 256, s, a);
     default: return cudaErrorInvalidValue;
@@ -80,7 +80,7 @@ cudaError_t launch_init(int precision, void* f0, void* f1, const uint8_t* cls, f
   switch (precision) {
     case AEROSIM_PREC_F32: AEROSIM_INIT(StoreF32S); break;
     case AEROSIM_PREC_F32_MIRROR: AEROSIM_INIT(StoreF32); break;
-    case AEROSIM_PREC_F16S: AEROSIM_INIT(StoreF16S); break;
+    case AEROSIM_PREC_F16S: case AEROSIM_PREC_F16C: AEROSIM_INIT(StoreF16S); break;
     case AEROSIM_PREC_BF16S: AEROSIM_INIT(StoreBF16S); break;
     case AEROSIM_PREC_F64: AEROSIM_INIT(StoreF64); break;
     default: return cudaErrorInvalidValue;
@@ -103,7 +103,7 @@ cudaError_t launch_read_pops(int precision, const void* f, const uint8_t* cls, c
   switch (precision) {
     case AEROSIM_PREC_F32: read_pops_t<StoreF32S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
     case AEROSIM_PREC_F32_MIRROR: read_pops_t<StoreF32, MODE_MIRROR>(f, cls, st, ps, L, N, out, dtype, s); break;
-    case AEROSIM_PREC_F16S: read_pops_t<StoreF16S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
+    case AEROSIM_PREC_F16S: case AEROSIM_PREC_F16C: read_pops_t<StoreF16S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
     case AEROSIM_PREC_BF16S: read_pops_t<StoreBF16S, MODE_FAST>(f, cls, st, ps, L, N, out, dtype, s); break;
     case AEROSIM_PREC_F64: read_pops_t<StoreF64, MODE_F64>(f, cls, st, ps, L, N, out, dtype, s); break;
     default: return cudaErrorInvalidValue;
@@ -124,7 +124,7 @@ cudaError_t launch_write_pops(int precision, void* f, const Layout& L, long long
   switch (precision) {
     case AEROSIM_PREC_F32: write_pops_t<StoreF32S>(f, L, N, in, dtype, s); break;
     case AEROSIM_PREC_F32_MIRROR: write_pops_t<StoreF32>(f, L, N, in, dtype, s); break;
-    case AEROSIM_PREC_F16S: write_pops_t<StoreF16S>(f, L, N, in, dtype, s); break;
+    case AEROSIM_PREC_F16S: case AEROSIM_PREC_F16C: write_pops_t<StoreF16S>(f, L, N, in, dtype, s); break;
     case AEROSIM_PREC_BF16S: write_pops_t<StoreBF16S>(f, L, N, in, dtype, s); break;
     case AEROSIM_PREC_F64: write_pops_t<StoreF64>(f, L, N, in, dtype, s); break;
     default: return cudaErrorInvalidValue;
@@ -138,7 +138,7 @@ cudaError_t launch_materialize(int precision, void* f, const uint8_t* cls, const
   switch (precision) {
     case AEROSIM_PREC_F32: materialize_rescale_kernel<StoreF32S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     case AEROSIM_PREC_F32_MIRROR: materialize_rescale_kernel<StoreF32, MODE_MIRROR><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
-    case AEROSIM_PREC_F16S: materialize_rescale_kernel<StoreF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
+    case AEROSIM_PREC_F16S: case AEROSIM_PREC_F16C: materialize_rescale_kernel<StoreF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     case AEROSIM_PREC_BF16S: materialize_rescale_kernel<StoreBF16S, MODE_FAST><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     case AEROSIM_PREC_F64: materialize_rescale_kernel<StoreF64, MODE_F64><<<g, 256, 0, s>>>(f, cls, st, ps, L, N); break;
     default: return cudaErrorInvalidValue;

@@ -11,6 +11,8 @@ cudaError_t launch_step_fast_f16s(const StepArgs& a, dim3 block, unsigned grid, 
                                   int* occ, int* launches);
 cudaError_t launch_step_fast_bf16s(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s,
                                    int* occ, int* launches);
+cudaError_t launch_step_fast_f16c(const StepArgs& a, dim3 block, unsigned grid, size_t smem, cudaStream_t s,
+                                  int* occ, int* launches);
 
 cudaError_t launch_batch_fast_f32(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
                                   int* occ);
@@ -18,6 +20,8 @@ cudaError_t launch_batch_fast_f16s(const BatchArgs& b, int pitch, unsigned grid,
                                    int* occ);
 cudaError_t launch_batch_fast_bf16s(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
                                     int* occ);
+cudaError_t launch_batch_fast_f16c(const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
+                                   int* occ);
 
 cudaError_t launch_batch(int precision, const BatchArgs& b, int pitch, unsigned grid, size_t smem, cudaStream_t s,
                          int* occ) {
@@ -25,6 +29,7 @@ cudaError_t launch_batch(int precision, const BatchArgs& b, int pitch, unsigned 
     case AEROSIM_PREC_F32: return launch_batch_fast_f32(b, pitch, grid, smem, s, occ);
     case AEROSIM_PREC_F16S: return launch_batch_fast_f16s(b, pitch, grid, smem, s, occ);
     case AEROSIM_PREC_BF16S: return launch_batch_fast_bf16s(b, pitch, grid, smem, s, occ);
+    case AEROSIM_PREC_F16C: return launch_batch_fast_f16c(b, pitch, grid, smem, s, occ);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -35,6 +40,7 @@ cudaError_t launch_step_fast(int precision, const StepArgs& a, dim3 block, unsig
     case AEROSIM_PREC_F32: return launch_step_fast_f32(a, block, grid, smem, s, occ, launches);
     case AEROSIM_PREC_F16S: return launch_step_fast_f16s(a, block, grid, smem, s, occ, launches);
     case AEROSIM_PREC_BF16S: return launch_step_fast_bf16s(a, block, grid, smem, s, occ, launches);
+    case AEROSIM_PREC_F16C: return launch_step_fast_f16c(a, block, grid, smem, s, occ, launches);
     default: return cudaErrorInvalidValue;
   }
 }

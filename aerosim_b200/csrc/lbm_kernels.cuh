@@ -636,11 +636,20 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, const void* fs
     const double2 ui = inlet_u(iy);
     const double uxi = ui.x, uyi = ui.y;
     const double ri = MODE == MODE_FAST ? (double)(0.85f * (float)mr + 0.15f) : 0.85 * (double)mr + 0.15 * 1.0;
+    if constexpr (S::kCompensate) {
+      float q[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) {
-      if constexpr (MODE == MODE_FAST)
-        blk[slot_of(d) * pitch] = S::raw_of_h(heq32(d, (float)ri, (float)uxi, (float)uyi, 0.f), d);
-      else blk[slot_of(d) * pitch] = S::raw_of_f(feq64(d, ri, uxi, uyi, 0.0), d);
+      for (int d = 0; d < 19; ++d) q[d] = S::kOutScale * heq32(d, (float)ri, (float)uxi, (float)uyi, 0.f);
+      compensate_cell<S>(q);
+#pragma unroll
+      for (int d = 0; d < 19; ++d) blk[slot_of(d) * pitch] = S::store(q[d]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) {
+        if constexpr (MODE == MODE_FAST)
+          blk[slot_of(d) * pitch] = S::raw_of_h(heq32(d, (float)ri, (float)uxi, (float)uyi, 0.f), d);
+        else blk[slot_of(d) * pitch] = S::raw_of_f(feq64(d, ri, uxi, uyi, 0.0), d);
+      }
     }
     if (write_macro) {
       a.mux[ic] = (float)uxi; a.muy[ic] = (float)uyi; a.muz[ic] = 0.0f; a.mrho[ic] = (float)(Mac)ri;
@@ -654,10 +663,20 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, const void* fs
     Mac ro;
     if constexpr (MODE == MODE_FAST) {
       const float r2 = (float)mr * 0.85f + 0.15f;
+      if constexpr (S::kCompensate) {
+        float q[19];
 #pragma unroll
-      for (int d = 0; d < 19; ++d)
-        out[slot_of(d) * pitch] =
-            S::raw_of_h(0.75f * v[d] + 0.25f * heq32(d, r2, (float)mx, (float)my, (float)mz), d);
+        for (int d = 0; d < 19; ++d)
+          q[d] = S::kOutScale * (0.75f * v[d] + 0.25f * heq32(d, r2, (float)mx, (float)my, (float)mz));
+        compensate_cell<S>(q);
+#pragma unroll
+        for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::store(q[d]);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 19; ++d)
+          out[slot_of(d) * pitch] =
+              S::raw_of_h(0.75f * v[d] + 0.25f * heq32(d, r2, (float)mx, (float)my, (float)mz), d);
+      }
       ro = (Mac)r2;
     } else {
       const double r2 = (double)mr * 0.85 + 1.0 * 0.15;
@@ -684,10 +703,19 @@ __device__ __forceinline__ long long near_cell(const StepArgs& a, const void* fs
     wall_feq<S, MODE>(v, (double)mr, (double)mx, (double)my, (double)mz);
   }
   T* out = blk + ix;
+  if constexpr (S::kCompensate) {
+    float q[19];
 #pragma unroll
-  for (int d = 0; d < 19; ++d) {
-    if constexpr (MODE == MODE_FAST) out[slot_of(d) * pitch] = S::raw_of_h(v[d], d);
-    else out[slot_of(d) * pitch] = S::raw_of_f(v[d], d);
+    for (int d = 0; d < 19; ++d) q[d] = S::kOutScale * v[d];
+    compensate_cell<S>(q);
+#pragma unroll
+    for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::store(q[d]);
+  } else {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+      if constexpr (MODE == MODE_FAST) out[slot_of(d) * pitch] = S::raw_of_h(v[d], d);
+      else out[slot_of(d) * pitch] = S::raw_of_f(v[d], d);
+    }
   }
   if (write_macro) {
     a.mux[cell] = (float)mx; a.muy[cell] = (float)my; a.muz[cell] = (float)mz; a.mrho[cell] = (float)mr;
@@ -866,11 +894,13 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
     if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
       const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
       const float2 ui = inlet_u(g.iy);
+      float q = 0.0f;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        const float h = heq_lane(cw, ri, ui.x, ui.y, 0.0f);
-        blk[s_dslot[lane] * pitch] = S::store(fmaf(S::kOutScale, h, S::kOutW * cw.w));
+        q = fmaf(S::kOutScale, heq_lane(cw, ri, ui.x, ui.y, 0.0f), S::kOutW * cw.w);
       }
+      q = compensate_lanes<S>(q, lane);
+      if (lane < 19) blk[s_dslot[lane] * pitch] = S::store(q);
       if (lane == 0) {
         if (ri == ri) my_sum += rho_fixed(ri);
         else my_nan = 1;
@@ -900,13 +930,16 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
       __syncwarp();
       const float ro = (stale ? 1.0f : r2) * 0.85f + 0.15f;
       const float mx = stale ? 0.0f : ox, my = stale ? 0.0f : oy, mz = stale ? 0.0f : oz;
+      float q = 0.0f;
+      const int sl = lane < 19 ? s_dslot[lane] : 0;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        const int sl = s_dslot[lane];
         const float h = heq_lane(cw, ro, mx, my, mz);
         const float prev = stale ? (float)blk[sl * pitch + nx - 2] : xo[sl];
-        blk[sl * pitch + nx - 1] = S::store(0.75f * prev + 0.25f * fmaf(S::kOutScale, h, S::kOutW * cw.w));
+        q = 0.75f * prev + 0.25f * fmaf(S::kOutScale, h, S::kOutW * cw.w);
       }
+      q = compensate_lanes<S>(q, lane);
+      if (lane < 19) blk[sl * pitch + nx - 1] = S::store(q);
       __syncwarp();
       if (lane == 0) {
         if (ro == ro) my_sum += rho_fixed(ro);
@@ -930,6 +963,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
   }
   if (own) {
     T* out = blk + ix;
+    compensate_cell<S>(v);
 #pragma unroll
     for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::store(v[d]);
     if (r == r) my_sum += rho_fixed(r);
@@ -1022,7 +1056,34 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
     heq_pair<S>(v, r, ux, uy, uz);
   }
   T* out = blk + x0;
-  if (own0 && own1) {
+  if constexpr (S::kCompensate) {
+    // mass-compensated rounding (compensate_cell) of both cells: the moving directions
+    // round first, as packed half2 that are kept for the stores, and direction 0 takes
+    // what their rounded values leave of the cell's deviation sum.  The collision and the
+    // wall equilibrium both conserve the density, so the 19 values sum to
+    // kOutScale (r - 1) (kOutW is 0 for the shifted codecs): direction 0 is formed from
+    // that sum rather than from its own value plus the rounding errors, which needs no
+    // second copy of the 18 values
+    static_assert(std::is_same<T, __half>::value && OW == 0.0f, "compensated rounding is a shifted FP16 codec");
+    __half2 hv[19];
+    float2 sr = f2(0.0f);
+#pragma unroll
+    for (int d = 1; d < 19; ++d) {
+      hv[d] = __float22half2_rn(v[d]);
+      sr = f2add(sr, __half22float2(hv[d]));
+    }
+    hv[0] = __float22half2_rn(f2sub(f2mul(f2(OS), f2sub(r, f2(1.0f))), sr));
+    if (own0 && own1) {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) *reinterpret_cast<__half2*>(out + slot_of(d) * pitch) = hv[d];
+    } else if (own0 || own1) {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) {
+        if (own0) out[slot_of(d) * pitch] = __low2half(hv[d]);
+        if (own1) out[slot_of(d) * pitch + 1] = __high2half(hv[d]);
+      }
+    }
+  } else if (own0 && own1) {
 #pragma unroll
     for (int d = 0; d < 19; ++d) store_pair<S>(out + slot_of(d) * pitch, v[d]);
   } else if (own0 || own1) {
@@ -1063,10 +1124,13 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
     if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
       const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
       const float2 ui = inlet_u(g.iy);
+      float q = 0.0f;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        blk[s_dslot[lane] * pitch] = S::store(fmaf(OS, heq_lane(cw, ri, ui.x, ui.y, 0.0f), OW * cw.w));
+        q = fmaf(OS, heq_lane(cw, ri, ui.x, ui.y, 0.0f), OW * cw.w);
       }
+      q = compensate_lanes<S>(q, lane);
+      if (lane < 19) blk[s_dslot[lane] * pitch] = S::store(q);
       if (lane == 0) {
         if (ri == ri) my_sum += rho_fixed(ri);
         else my_nan = 1;
@@ -1087,13 +1151,15 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
       __syncwarp();
       const float ro = (stale ? 1.0f : xo[19]) * 0.85f + 0.15f;
       const float mx = stale ? 0.0f : xo[20], my = stale ? 0.0f : xo[21], mz = stale ? 0.0f : xo[22];
+      float q = 0.0f;
+      const int sl = lane < 19 ? s_dslot[lane] : 0;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        const int sl = s_dslot[lane];
         const float prev = stale ? S::raw(blk[sl * pitch + nx - 2]) : xo[sl];
-        blk[sl * pitch + nx - 1] =
-            S::store(0.75f * prev + 0.25f * fmaf(OS, heq_lane(cw, ro, mx, my, mz), OW * cw.w));
+        q = 0.75f * prev + 0.25f * fmaf(OS, heq_lane(cw, ro, mx, my, mz), OW * cw.w);
       }
+      q = compensate_lanes<S>(q, lane);
+      if (lane < 19) blk[sl * pitch + nx - 1] = S::store(q);
       __syncwarp();  // the scratch row is free for the next segment
       if (lane == 0) {
         if (ro == ro) my_sum += rho_fixed(ro);

@@ -15,7 +15,7 @@
    last one is held out: the closure's eddy viscosity and Smagorinsky's are both scored
    against the filtered subgrid stress (mean squared error of nu_t / nu_0).
 3. Coarse runs at 256x128x128 over the same physical time (half the steps): plain
-   Smagorinsky and the learned closure.  Cd over the second half of each run against the
+   Smagorinsky, the learned closure and no eddy viscosity at all.  Cd over the second half of each run against the
    fine run's (with the standard error of each mean from 10 block means), and device time
    of each run.
 
@@ -34,11 +34,12 @@ import numpy as np
 from . import LBMEngine, cases, frontal_area, sgs
 
 
-def _engine(case, precision: str = "f32") -> LBMEngine:
+def _engine(case, precision: str = "f32", cs: float | None = None) -> LBMEngine:
     pos = case.mesh[0]
     e = LBMEngine(0)
     e.voxelize(case.mesh, None, case.tunnel, {"nx": case.nx, "ny": case.ny, "nz": case.nz},
-               {"uInletLattice": case.u_inlet, "nuLattice": case.nu, "smagorinskyCs": case.cs,
+               {"uInletLattice": case.u_inlet, "nuLattice": case.nu,
+                "smagorinskyCs": case.cs if cs is None else cs,
                 "precision": precision, "frontalAreaM2": frontal_area(case.mesh),
                 "characteristicLengthM": float(pos[:, 0].max() - pos[:, 0].min())})
     return e
@@ -135,8 +136,11 @@ def main(argv=None) -> dict:
 
     # ---- 3. coarse runs: plain and learned closure ----
     steps_c = a.fine_steps // 2
-    for name, params in (("coarse_smagorinsky", None), ("coarse_mlp", p)):
-        e = _engine(coarse_case)
+    # coarse_no_model: no eddy viscosity at all (Cs = 0, the molecular tau with the
+    # reference's clamp): how much of the coarse Cd error any viscosity model can act on
+    for name, params, cs in (("coarse_smagorinsky", None, None), ("coarse_mlp", p, None),
+                             ("coarse_no_model", None, 0.0)):
+        e = _engine(coarse_case, cs=cs)
         if params is not None:
             e.set_sgs_mlp(params)
         cd, ms = _run(e, steps_c, 100)

@@ -213,7 +213,7 @@ def run_ours(args) -> dict:
     eng.close()
 
     # ---- FP16 / BF16 shifted storage: throughput ----
-    for prec in [p for p in args.precisions.split(",") if p in ("f16s", "bf16s")]:
+    for prec in [p for p in args.precisions.split(",") if p in ("f16s", "bf16s", "f16c")]:
         e2, _ = _make_engine(case, prec, dev)
         e2.step(args.warmup)
         barrier_sync()
@@ -256,8 +256,9 @@ def run_ours(args) -> dict:
             "vs_smagorinsky_time": round((ms4 / args.sgs_steps) / (ms / args.steps), 3), "gpu_launches": int(l4),
             "nan": nan, "inference": "BF16 mma.sync m16n8k16 tiles, FP32 accumulation, inside the step kernel",
             "in_step_paths": in_step,
-            "training": {k: meta[k] for k in ("fine", "coarse", "fine_cd_mean", "heldout_mse_mlp",
-                                               "heldout_mse_smagorinsky", "coarse_smagorinsky", "coarse_mlp")
+            "training": {k: meta[k] for k in ("fine", "coarse", "fine_steps", "fine_cd_mean", "fine_cd_se",
+                                               "heldout_mse_mlp", "heldout_mse_smagorinsky", "coarse_smagorinsky",
+                                               "coarse_mlp", "coarse_no_model")
                          if k in meta},
             "forward_tiles": closure_forward_tiles(w["params"], cells)}
 
@@ -319,7 +320,7 @@ def _cd_series(case, prec: str, steps: int, every: int, dev: int, perturb: float
 
 
 def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True,
-               precisions=("f32", "f16s", "bf16s"), control: bool = True) -> dict:
+               precisions=("f32", "f16s", "bf16s", "f16c"), control: bool = True) -> dict:
     """Cd / Cl / Cm of every storage mode against the FP64 GPU run (FP64 populations and
     arithmetic).  The flow at Re = 2e4 is unsteady and chaotic: runs that differ only in
     rounding follow each other for the first few thousand steps and then decorrelate.
@@ -374,7 +375,7 @@ def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True
         from aerosim_b200 import cases
         sph = cases.sphere_64x32x32()
         vals = {}
-        for prec in ("f64", "f32", "f16s", "bf16s"):
+        for prec in ("f64", *precisions):
             e5, _ = _make_engine(sph, prec, dev)
             e5.step(3500)
             cds = []
@@ -385,7 +386,7 @@ def cd_vs_fp64(case, steps: int, dev: int, blocks: int = 10, steady: bool = True
             e5.close()
         summary["steady_sphere_re100"] = {
             "case": "sphere_64x32x32, u 0.05, Re 100, Cd mean of steps 3500..4000", "cd_f64": vals["f64"],
-            **{f"dcd_rel_{p}": abs(vals[p] - vals["f64"]) / abs(vals["f64"]) for p in ("f32", "f16s", "bf16s")}}
+            **{f"dcd_rel_{p}": abs(vals[p] - vals["f64"]) / abs(vals["f64"]) for p in precisions}}
     return summary
 
 
@@ -541,8 +542,8 @@ def main():
                     help="steps of the batched 32-wing sweep (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI frame loop")
-    ap.add_argument("--precisions", default="f32,f16s,bf16s",
-                    help="storage modes timed after the FP32 headline (f16s, bf16s)")
+    ap.add_argument("--precisions", default="f32,f16s,bf16s,f16c",
+                    help="storage modes timed after the FP32 headline (f16s, bf16s, f16c)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

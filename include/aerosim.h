@@ -49,7 +49,9 @@ enum aerosim_precision {
                                   reference's JavaScript CPU solver (bit-parity mode) */
   AEROSIM_PREC_F16S = 2,       /* FP16 storage of (f - w) scaled by 2^15, FP32 collision */
   AEROSIM_PREC_BF16S = 3,      /* BF16 storage of (f - w), FP32 collision */
-  AEROSIM_PREC_F64 = 4         /* FP64 storage and arithmetic (the GPU FP64 oracle run) */
+  AEROSIM_PREC_F64 = 4,        /* FP64 storage and arithmetic (the GPU FP64 oracle run) */
+  AEROSIM_PREC_F16C = 5        /* F16S values with mass-compensated rounding: the rounding errors of a
+                                  cell's 18 moving populations go into its rest population */
 };
 
 /* Element type for population read/write. */
