@@ -10,8 +10,9 @@ input: the mesh is generated from a fixed seed; no dataset is read.
 Prints one JSON line (rank 0).  `value` is whole-job MLUPS measured with CUDA events
 around exactly K steps (inputs resident in HBM; the populations, 637 MB, exceed the
 126 MB L2, so no flush is needed).  `e2e` is the same metric through the C-ABI frame
-loop of the reference's solver interface: aerosim_step(4 substeps) followed by the
-force readout to the host, timed on the host clock.  Under torchrun every rank runs
+call of the reference's solver interface, aerosim_step_and_extract_slice (stepAndExtractSlice:
+4 substeps, the FP64 force sums and the z = nz/2 velocity slice copied into host buffers),
+timed on the host clock; `e2e.python_api_mlups` is the same loop through the Python engine.  Under torchrun every rank runs
 its own lattice (independent shards, weak scaling); times are the max over ranks.
 
 --impl reference times the reference algorithm's CPU implementation on the host
@@ -56,8 +57,9 @@ def _peaks():
 
 def _profile_traffic(precision: str):
     """DRAM bytes per step-kernel launch from the committed ncu summary, if any."""
-    name = ("main_kernel_ellipsoid_256x128x128.md" if precision == "f32"
-            else "main_kernel_f16s_pairs_ellipsoid_256x128x128.md")
+    name = {"f32": "main_kernel_ellipsoid_256x128x128.md",
+            "f16c": "main_kernel_f16c_pairs_ellipsoid_256x128x128.md"}.get(
+        precision, "main_kernel_f16s_pairs_ellipsoid_256x128x128.md")
     path = os.path.join(ROOT, "profiles", name)
     try:
         text = open(path).read()
@@ -185,21 +187,38 @@ def run_ours(args) -> dict:
         "boundary_cells": int(info.boundary_cell_count), "solid_cells": int(info.solid_cell_count),
     })
 
-    # ---- e2e: frames of 4 substeps + force readout to the host through the C-ABI ----
+    # ---- e2e: frames of 4 substeps + forces + slice image into host buffers, C-ABI ----
     frames = max(4, args.steps // 4) if not args.no_e2e else 0
     if frames:
-        sl = {"axis": "z", "fraction": 0.5, "mode": "velocity"}
+        import ctypes
+        lib, hnd = N.load(), eng._h.h
+        fw, fh, fr = ctypes.c_int32(), ctypes.c_int32(), N.Forces()
+        N.check(lib.aerosim_extract_slice(hnd, 2, 0.5, 0, None, ctypes.byref(fw), ctypes.byref(fh)))
+        rgba = np.empty(fw.value * fh.value * 4, np.uint8)  # the host's image buffer, reused per frame
+
+        def frame():
+            N.check(lib.aerosim_step_and_extract_slice(hnd, 4, 2, 0.5, 0, N.ptr(rgba, ctypes.c_uint8),
+                                                       ctypes.byref(fw), ctypes.byref(fh), ctypes.byref(fr)))
+
         for _ in range(2):
-            eng.step_and_extract_slice(4, slice=sl)
+            frame()
         barrier_sync()
         t0 = time.perf_counter()
         for _ in range(frames):
-            fr = eng.step_and_extract_slice(4, slice=sl)
+            frame()
         dt = time.perf_counter() - t0
         barrier_sync()
         dt = max_over_ranks(dt)
-        import ctypes
-        frame_d2h = ctypes.sizeof(N.Forces) + 4 + fr["rgba"].nbytes
+        sl = {"axis": "z", "fraction": 0.5, "mode": "velocity"}  # the same frames through the Python engine
+        eng.step_and_extract_slice(4, slice=sl)
+        barrier_sync()
+        t1 = time.perf_counter()
+        for _ in range(frames):
+            eng.step_and_extract_slice(4, slice=sl)
+        dt_py = time.perf_counter() - t1
+        barrier_sync()
+        dt_py = max_over_ranks(dt_py)
+        frame_d2h = ctypes.sizeof(N.Forces) + 4 + rgba.nbytes
         # per step, the solver parameters (step index, inlet velocity, tau, buffers) travel
         # host -> device as the step kernel's argument block, where the reference uploads
         # its 48-byte SolverParams uniform before every substep (lbmEngine.ts:330-354)
@@ -209,7 +228,8 @@ def run_ours(args) -> dict:
                       "h2d": "step kernel argument block (solver parameters of the step) per launch",
                       "frame": "stepAndExtractSlice: aerosim_step_and_extract_slice (4 substeps, FP64 force sums, "
                                "z = nz/2 velocity RGBA slice, one synchronization), results copied to the host",
-                      "frames": frames}
+                      "frames": frames,
+                      "python_api_mlups": round(ws * cells * 4 * frames / dt_py / 1e6, 1)}
     eng.close()
 
     # ---- FP16 / BF16 shifted storage: throughput ----
