@@ -1056,6 +1056,13 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
     heq_pair<S>(v, r, ux, uy, uz);
   }
   T* out = blk + x0;
+  // A row end (cell 0 or nx-1) that this warp rewrites below -- the inlet or the outlet,
+  // after a __syncwarp that orders the warp's global stores -- takes the pair store with
+  // its neighbour, so the lanes of a row-end segment all store pairs instead of
+  // diverging into per-cell stores.  Not for a solid row end (never written) nor with a
+  // near-wall neighbour (the near-wall pass writes the row end then).
+  const bool pair_st = (own0 && own1) || (own1 && x0 == 0 && f0 != CELL_SOLID) ||
+                       (own0 && x0 + 1 == nx - 1 && f1 != CELL_SOLID);
   if constexpr (S::kCompensate) {
     // mass-compensated rounding (compensate_cell) of both cells: the moving directions
     // round first, as packed half2 that are kept for the stores, and direction 0 takes
@@ -1073,7 +1080,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
       sr = f2add(sr, __half22float2(hv[d]));
     }
     hv[0] = __float22half2_rn(f2sub(f2mul(f2(OS), f2sub(r, f2(1.0f))), sr));
-    if (own0 && own1) {
+    if (pair_st) {
 #pragma unroll
       for (int d = 0; d < 19; ++d) *reinterpret_cast<__half2*>(out + slot_of(d) * pitch) = hv[d];
     } else if (own0 || own1) {
@@ -1083,7 +1090,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
         if (own1) out[slot_of(d) * pitch + 1] = __high2half(hv[d]);
       }
     }
-  } else if (own0 && own1) {
+  } else if (pair_st) {
 #pragma unroll
     for (int d = 0; d < 19; ++d) store_pair<S>(out + slot_of(d) * pitch, v[d]);
   } else if (own0 || own1) {
@@ -1130,6 +1137,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
         q = fmaf(OS, heq_lane(cw, ri, ui.x, ui.y, 0.0f), OW * cw.w);
       }
       q = compensate_lanes<S>(q, lane);
+      __syncwarp();  // after lane 0's pair store of cells 0 and 1
       if (lane < 19) blk[s_dslot[lane] * pitch] = S::store(q);
       if (lane == 0) {
         if (ri == ri) my_sum += rho_fixed(ri);
@@ -1148,7 +1156,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
     const int c2 = __shfl_sync(0xffffffffu, (int)g.c0, src), c3 = __shfl_sync(0xffffffffu, (int)g.c1, src);
     const bool stale = (c2 & CLS_FLAG_MASK) == CELL_SOLID;
     if ((c3 & CLS_FLAG_MASK) != CELL_SOLID && !((c2 & CLS_NEAR) && !stale)) {
-      __syncwarp();
+      __syncwarp();  // the parked row xo, and the pair store of cells nx-2 and nx-1 before ours
       const float ro = (stale ? 1.0f : xo[19]) * 0.85f + 0.15f;
       const float mx = stale ? 0.0f : xo[20], my = stale ? 0.0f : xo[21], mz = stale ? 0.0f : xo[22];
       float q = 0.0f;
