@@ -535,8 +535,11 @@ __host__ __device__ inline size_t step_smem_bytes(const Layout& L, int stages, s
 // outlet (:323-373), store.  Meanwhile the helper warp takes the CTA's share of the
 // near-wall cells (Bouzidi, :196-221; one lane per cell from a link table built with
 // the voxel grid).  A near-wall cell at ix = 1 or nx-2 carries its row's inlet or
-// outlet, which need its post-collision values.  The last CTA takes the step's
-// mean-density rescale decision (:431-455).
+// outlet, which need its post-collision values.  With 16-bit storage and two cells per
+// thread the helper warp also takes, from every ring slot, the two pairs of each row
+// that hold its ends (end_pair; the consumers leave them out), and a batch of near-wall
+// cells after each slot.  The last CTA takes the step's mean-density rescale decision
+// (:431-455).
 //
 // P is the row pitch when it is a compile-time constant (0: L.pitch at run time):
 // with a constant pitch every shared-memory load and global store of a cell is an
@@ -840,12 +843,51 @@ __device__ __forceinline__ long long general_cells(const StepArgs& a, double (&v
   return add;
 }
 
-// Equilibrium deviation of a run-time direction (the lane-transposed row ends):
-// c = (c_x, c_y, c_z), w the float weight.
+// The row ends' equilibria round every operation explicitly (FMA forms), so that the
+// lane-transposed row ends (a run-time direction per lane) and the helper warp's end
+// pairs (end_pair, unrolled directions) give the same bits: w_d ((rho - 1) + rho k) with
+// k = cu + cu^2 / 2 - 1.5 u^2, cu = 3 c_d . u.  The run-time dot product adds the zero
+// products c_a u_a = +-0 that dotc leaves out, which changes no sum but the sign of a
+// zero, and that sign does not reach the result.
+__device__ __forceinline__ float usq_of(float ux, float uy, float uz) {
+  return __fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz)));
+}
+__device__ __forceinline__ float heq_of_dot(float dot, float w, float rho, float usq) {
+  const float cu = __fmul_rn(3.0f, dot);
+  const float k = __fmaf_rn(-1.5f, usq, __fmaf_rn(__fmul_rn(0.5f, cu), cu, cu));
+  return __fmul_rn(w, __fmaf_rn(rho, k, __fsub_rn(rho, 1.0f)));
+}
+// Equilibrium deviation feq - w of a run-time direction c = (c_x, c_y, c_z, w).
 __device__ __forceinline__ float heq_lane(const float4 c, float rho, float ux, float uy, float uz) {
-  const float cu = 3.0f * (c.x * ux + c.y * uy + c.z * uz);
-  const float uSq = ux * ux + uy * uy + uz * uz;
-  return c.w * ((rho - 1.0f) + rho * (cu + 0.5f * cu * cu - 1.5f * uSq));
+  const float dot = __fadd_rn(__fadd_rn(__fmul_rn(c.x, ux), __fmul_rn(c.y, uy)), __fmul_rn(c.z, uz));
+  return heq_of_dot(dot, c.w, rho, usq_of(ux, uy, uz));
+}
+// The row ends' density from their source cell's: 0.85 rho + 0.15 (:336, :358).
+__device__ __forceinline__ float end_rho(float r) { return __fmaf_rn(0.85f, r, 0.15f); }
+// Inlet value in the storage domain from the equilibrium deviation h of weight w (:343-350).
+template <class S>
+__device__ __forceinline__ float inlet_value(float h, float w) {
+  return __fmaf_rn(S::kOutScale, h, S::kOutW * w);
+}
+// Outlet value: 0.75 of the source cell's post-collision value plus 0.25 of the
+// equilibrium of its moments (:361-368).
+template <class S>
+__device__ __forceinline__ float outlet_value(float prev, float h, float w) {
+  return __fmaf_rn(0.75f, prev, __fmul_rn(0.25f, __fmaf_rn(S::kOutScale, h, S::kOutW * w)));
+}
+// compensate_lanes' correction as lane 0 sums it (the butterfly's order), for a cell whose
+// 19 values one thread holds: the rounding errors of directions 1..18.
+template <class S>
+__device__ __forceinline__ float lane_order_errors(const float (&q)[19]) {
+  float e[32];
+#pragma unroll
+  for (int l = 0; l < 32; ++l) e[l] = (l >= 1 && l < 19) ? q[l] - S::raw(S::store(q[l])) : 0.0f;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int l = 0; l < o; ++l) e[l] = e[l] + e[l + o];
+  }
+  return e[0];
 }
 
 // One FP32-arithmetic consumer segment (32 cells of an x-row), shared by the
@@ -892,12 +934,12 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
     const float r1 = __shfl_sync(0xffffffffu, r, 1 - cell_lo);
     const bool solid1 = (c1 & CLS_FLAG_MASK) == CELL_SOLID;
     if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
-      const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
+      const float ri = end_rho(solid1 ? 1.0f : r1);
       const float2 ui = inlet_u(g.iy);
       float q = 0.0f;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        q = fmaf(S::kOutScale, heq_lane(cw, ri, ui.x, ui.y, 0.0f), S::kOutW * cw.w);
+        q = inlet_value<S>(heq_lane(cw, ri, ui.x, ui.y, 0.0f), cw.w);
       }
       q = compensate_lanes<S>(q, lane);
       if (lane < 19) blk[s_dslot[lane] * pitch] = S::store(q);
@@ -928,15 +970,14 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
         for (int d = 0; d < 19; ++d) xo[slot_of(d)] = v[d];
       }
       __syncwarp();
-      const float ro = (stale ? 1.0f : r2) * 0.85f + 0.15f;
+      const float ro = end_rho(stale ? 1.0f : r2);
       const float mx = stale ? 0.0f : ox, my = stale ? 0.0f : oy, mz = stale ? 0.0f : oz;
       float q = 0.0f;
       const int sl = lane < 19 ? s_dslot[lane] : 0;
       if (lane < 19) {
-        const float4 cw = s_dcw[lane];
-        const float h = heq_lane(cw, ro, mx, my, mz);
         const float prev = stale ? (float)blk[sl * pitch + nx - 2] : xo[sl];
-        q = 0.75f * prev + 0.25f * fmaf(S::kOutScale, h, S::kOutW * cw.w);
+        const float4 cw = s_dcw[lane];
+        q = outlet_value<S>(prev, heq_lane(cw, ro, mx, my, mz), cw.w);
       }
       q = compensate_lanes<S>(q, lane);
       if (lane < 19) blk[sl * pitch + nx - 1] = S::store(q);
@@ -1026,7 +1067,10 @@ struct PairGeom {
 // warp's scratch row xo[24].  After the cells' own stores the warp holding a row end writes
 // it lane-transposed (lane d writes direction d), so the row-end work is one equilibrium
 // per lane and not 19 per thread, whether the compiler branches around it or predicates it.
-template <class S, class InletFn>
+// ENDS = false: the two pairs of the row that hold its ends, (0, 1) and (nx-2, nx-1), are
+// left out altogether (no stores, density sums or macros) -- the helper warp computes
+// them from the same ring slot (end_pair) -- and the segment carries no row-end code.
+template <class S, class InletFn, bool ENDS = true>
 __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __restrict__ fd, const PairGeom g,
                                              float tau0, float k_smag, float2 dec, InletFn inlet_u,
                                              const StepArgs& m, float* xo, const float4* s_dcw,
@@ -1039,9 +1083,10 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
   float2 r, ux, uy, uz;
   collide_fast2<S>(v, r, ux, uy, uz, tau0, k_smag, dec);  // v: storage domain
   const int f0 = g.c0 & CLS_FLAG_MASK, f1 = g.c1 & CLS_FLAG_MASK;
-  const bool own0 = g.active && f0 != CELL_SOLID && !(g.c0 & CLS_NEAR) && x0 != 0;
-  const bool own1 = g.active && f1 != CELL_SOLID && !(g.c1 & CLS_NEAR) && x0 + 1 != nx - 1;
-  if (g.has_hi && x0 == nx - 2) {  // the outlet's sources
+  const bool mine = ENDS || (x0 != 0 && x0 + 2 != nx);  // not a pair of the helper warp
+  const bool own0 = mine && g.active && f0 != CELL_SOLID && !(g.c0 & CLS_NEAR) && x0 != 0;
+  const bool own1 = mine && g.active && f1 != CELL_SOLID && !(g.c1 & CLS_NEAR) && x0 + 1 != nx - 1;
+  if (ENDS && g.has_hi && x0 == nx - 2) {  // the outlet's sources
 #pragma unroll
     for (int d = 0; d < 19; ++d) xo[slot_of(d)] = v[d].x;
     xo[19] = r.x; xo[20] = ux.x; xo[21] = uy.x; xo[22] = uz.x;
@@ -1108,7 +1153,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
     if (r.y == r.y) my_sum += rho_fixed(r.y);
     else my_nan = 1;
   }
-  if (g.write_macro && g.active) {
+  if (g.write_macro && g.active && mine) {
     const long long di = row * nx + x0;
     if (f0 == CELL_SOLID) {  // solid macro (:173-179)
       m.mux[di] = 0.0f; m.muy[di] = 0.0f; m.muz[di] = 0.0f; m.mrho[di] = 1.0f;
@@ -1121,6 +1166,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
       m.mux[di + 1] = ux.y; m.muy[di + 1] = uy.y; m.muz[di + 1] = uz.y; m.mrho[di + 1] = r.y;
     }
   }
+  if constexpr (!ENDS) return;
   if (g.has_lo) {
     // inlet (:328-352) from the density of cell 1 (1 for a solid, :177; the walls leave
     // the density as it is), both held by lane 0; a near-wall cell 1 defers it to the
@@ -1129,12 +1175,12 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
     const float r1 = __shfl_sync(0xffffffffu, r.y, 0);
     const bool solid1 = (c1 & CLS_FLAG_MASK) == CELL_SOLID;
     if ((c0 & CLS_FLAG_MASK) != CELL_SOLID && !((c1 & CLS_NEAR) && !solid1)) {
-      const float ri = 0.85f * (solid1 ? 1.0f : r1) + 0.15f;
+      const float ri = end_rho(solid1 ? 1.0f : r1);
       const float2 ui = inlet_u(g.iy);
       float q = 0.0f;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        q = fmaf(OS, heq_lane(cw, ri, ui.x, ui.y, 0.0f), OW * cw.w);
+        q = inlet_value<S>(heq_lane(cw, ri, ui.x, ui.y, 0.0f), cw.w);
       }
       q = compensate_lanes<S>(q, lane);
       __syncwarp();  // after lane 0's pair store of cells 0 and 1
@@ -1157,14 +1203,14 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
     const bool stale = (c2 & CLS_FLAG_MASK) == CELL_SOLID;
     if ((c3 & CLS_FLAG_MASK) != CELL_SOLID && !((c2 & CLS_NEAR) && !stale)) {
       __syncwarp();  // the parked row xo, and the pair store of cells nx-2 and nx-1 before ours
-      const float ro = (stale ? 1.0f : xo[19]) * 0.85f + 0.15f;
+      const float ro = end_rho(stale ? 1.0f : xo[19]);
       const float mx = stale ? 0.0f : xo[20], my = stale ? 0.0f : xo[21], mz = stale ? 0.0f : xo[22];
       float q = 0.0f;
       const int sl = lane < 19 ? s_dslot[lane] : 0;
       if (lane < 19) {
-        const float4 cw = s_dcw[lane];
         const float prev = stale ? S::raw(blk[sl * pitch + nx - 2]) : xo[sl];
-        q = 0.75f * prev + 0.25f * fmaf(OS, heq_lane(cw, ro, mx, my, mz), OW * cw.w);
+        const float4 cw = s_dcw[lane];
+        q = outlet_value<S>(prev, heq_lane(cw, ro, mx, my, mz), cw.w);
       }
       q = compensate_lanes<S>(q, lane);
       if (lane < 19) blk[sl * pitch + nx - 1] = S::store(q);
@@ -1179,6 +1225,162 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
       }
     }
   }
+}
+
+// One component of heq_pair with the same operations, so that a cell's equilibrium
+// rounds as it would in the pair form: OS (feq_d - w_d) + OW w_d.
+template <class S>
+__device__ __forceinline__ float heq_one(int d, float r, float ux, float uy, float uz) {
+  constexpr float OS = S::kOutScale, OW = S::kOutW;
+  const float u2 = __fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz)));
+  const float A = __fmaf_rn(__fmul_rn(-1.5f, r), u2, __fsub_rn(r, 1.0f));
+  const float cu = __fmul_rn(3.0f, dotc(d, ux, uy, uz));
+  const float h = __fmaf_rn(r, __fmaf_rn(__fmul_rn(0.5f, cu), cu, cu), A);
+  return __fmaf_rn(OS * wf_of(d), h, OW * wf_of(d));
+}
+
+// A pair of an x-row that holds one of its ends: cells (0, 1) (x0 = 0) or (nx-2, nx-1).
+struct EndGeom {
+  long long row;
+  int nx, ny, nz, pitch;
+  int iy, iz, x0;
+  bool wall_row, ground_no_slip, write_macro;
+  uint8_t c0, c1;  // class bytes of the two cells
+};
+
+// The helper warp's share of a two-cells-per-thread step: one lane per row-end pair,
+// pulled from the ring slot like a consumer pair, with pair_segment's semantics for
+// both cells -- the collision of both, the inlet of cell 0 from the density of cell 1
+// (:328-352) or the outlet of cell nx-1 from the post-collision, pre-wall values of
+// cell nx-2 (:354-371), the wall condition of the pair's interior cell (:375-429), the
+// stores, the density sum and the macro outputs -- with the row end's 19 equilibria
+// evaluated in the lane itself.  A near-wall interior cell defers the row end to the
+// near-wall pass (near_cell writes both), a solid row end is never written.  Returns
+// the fixed-point density added to the step's sum.
+template <class S, class InletFn>
+__device__ __forceinline__ long long end_pair(float2 (&v)[19], typename S::T* __restrict__ fd, const EndGeom g,
+                                              float tau0, float k_smag, float2 dec, InletFn inlet_u,
+                                              const StepArgs& m, int& my_nan) {
+  using T = typename S::T;
+  constexpr float OS = S::kOutScale;
+  const int pitch = g.pitch;
+  const bool lo = g.x0 == 0;
+  T* const out = fd + g.row * 19 * pitch + g.x0;
+  float2 r, ux, uy, uz;
+  collide_fast2<S>(v, r, ux, uy, uz, tau0, k_smag, dec);  // v: storage domain
+  const int f0 = g.c0 & CLS_FLAG_MASK, f1 = g.c1 & CLS_FLAG_MASK;
+  // the interior cell (1 or nx-2), unless solid or near-wall
+  const bool own = lo ? (f1 != CELL_SOLID && !(g.c1 & CLS_NEAR)) : (f0 != CELL_SOLID && !(g.c0 & CLS_NEAR));
+  bool end = false;                              // the row end is written here
+  float er = 0.0f, eu = 0.0f, ev = 0.0f, ew = 0.0f;  // its density and velocity
+  if (lo) {
+    if (f0 != CELL_SOLID && !((g.c1 & CLS_NEAR) && f1 != CELL_SOLID)) {
+      er = end_rho(f1 == CELL_SOLID ? 1.0f : r.y);
+      const float2 ui = inlet_u(g.iy);
+      eu = ui.x;
+      ev = ui.y;
+      const float us = usq_of(eu, ev, 0.0f);
+#pragma unroll
+      for (int d = 0; d < 19; ++d)
+        v[d].x = inlet_value<S>(heq_of_dot(dotc(d, eu, ev, 0.0f), wf_of(d), er, us), wf_of(d));
+      end = true;
+    }
+  } else {
+    const bool stale = f0 == CELL_SOLID;  // fDst's values of a solid nx-2 (never written)
+    if (f1 != CELL_SOLID && !((g.c0 & CLS_NEAR) && !stale)) {
+      er = end_rho(stale ? 1.0f : r.x);
+      eu = stale ? 0.0f : ux.x;
+      ev = stale ? 0.0f : uy.x;
+      ew = stale ? 0.0f : uz.x;
+      const float us = usq_of(eu, ev, ew);
+#pragma unroll
+      for (int d = 0; d < 19; ++d) {
+        const float prev = stale ? S::raw(out[slot_of(d) * pitch]) : v[d].x;
+        v[d].y = outlet_value<S>(prev, heq_of_dot(dotc(d, eu, ev, ew), wf_of(d), er, us), wf_of(d));
+      }
+      end = true;
+    }
+  }
+  if (g.wall_row) {  // floor, ceiling, then sides, on the interior cell
+    if (g.iy == 0) {
+      if (g.ground_no_slip) { ux = f2(0.0f); uz = f2(0.0f); }
+      uy = f2(0.0f);
+    }
+    if (g.iy == g.ny - 1) uy = f2(0.0f);
+    if (g.nz > 4 && (g.iz == 0 || g.iz == g.nz - 1)) uz = f2(0.0f);
+    if (lo) {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) v[d].y = heq_one<S>(d, r.y, ux.y, uy.y, uz.y);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) v[d].x = heq_one<S>(d, r.x, ux.x, uy.x, uz.x);
+    }
+  }
+  const bool s0 = lo ? end : own, s1 = lo ? own : end;
+  if constexpr (S::kCompensate) {
+    // the interior cell's direction 0 from its deviation sum OS (r - 1) as in
+    // pair_segment, the row end's from its own value plus the moving directions'
+    // rounding errors, summed in compensate_lanes' order
+    static_assert(std::is_same<T, __half>::value, "compensated rounding is a shifted FP16 codec");
+    float q[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) q[d] = lo ? v[d].x : v[d].y;
+    const float q0 = q[0] + lane_order_errors<S>(q);
+    __half2 hv[19];
+    float2 sr = f2(0.0f);
+#pragma unroll
+    for (int d = 1; d < 19; ++d) {
+      hv[d] = __float22half2_rn(v[d]);
+      sr = f2add(sr, __half22float2(hv[d]));
+    }
+    const float ix = OS * (r.x - 1.0f) - sr.x, iy_ = OS * (r.y - 1.0f) - sr.y;
+    hv[0] = __floats2half2_rn(lo ? q0 : ix, lo ? iy_ : q0);
+    if (s0 && s1) {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) *reinterpret_cast<__half2*>(out + slot_of(d) * pitch) = hv[d];
+    } else if (s0) {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = __low2half(hv[d]);
+    } else if (s1) {
+#pragma unroll
+      for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch + 1] = __high2half(hv[d]);
+    }
+  } else if (s0 && s1) {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) store_pair<S>(out + slot_of(d) * pitch, v[d]);
+  } else if (s0) {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch] = S::store(v[d].x);
+  } else if (s1) {
+#pragma unroll
+    for (int d = 0; d < 19; ++d) out[slot_of(d) * pitch + 1] = S::store(v[d].y);
+  }
+  long long add = 0;
+  const float ri = lo ? r.y : r.x;
+  if (own) {
+    if (ri == ri) add += rho_fixed(ri);
+    else my_nan = 1;
+  }
+  if (end) {
+    if (er == er) add += rho_fixed(er);
+    else my_nan = 1;
+  }
+  if (g.write_macro) {
+    const long long di = g.row * g.nx + g.x0;
+    const float ru = lo ? ux.y : ux.x, rv = lo ? uy.y : uy.x, rw = lo ? uz.y : uz.x;
+    if (f0 == CELL_SOLID) {  // solid macro (:173-179)
+      m.mux[di] = 0.0f; m.muy[di] = 0.0f; m.muz[di] = 0.0f; m.mrho[di] = 1.0f;
+    } else if (s0) {
+      m.mux[di] = lo ? eu : ru; m.muy[di] = lo ? ev : rv; m.muz[di] = lo ? ew : rw; m.mrho[di] = lo ? er : ri;
+    }
+    if (f1 == CELL_SOLID) {
+      m.mux[di + 1] = 0.0f; m.muy[di + 1] = 0.0f; m.muz[di + 1] = 0.0f; m.mrho[di + 1] = 1.0f;
+    } else if (s1) {
+      m.mux[di + 1] = lo ? ru : eu; m.muy[di + 1] = lo ? rv : ev; m.muz[di + 1] = lo ? rw : ew;
+      m.mrho[di + 1] = lo ? ri : er;
+    }
+  }
+  return add;
 }
 
 // CPT: consumer cells per thread, 1 or 2 (MODE_FAST without the closure, even nx; the
@@ -1251,6 +1453,11 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP, CP
   // divide the 8 consumer warps (row spans of 96, 160, 192, 224 threads) the
   // remaining warps take no rows.
   const int n_cons = RY * wpr;
+  // Two cells per thread: the helper warp takes the row-end pairs of every item from the
+  // ring (end_pair) and releases each slot with the consumers.
+  // (16-bit storage only: the FP32 steps, bound by bandwidth, lose more to the helper's
+  // slot releases than they gain: 101.4 -> 106.9 us at 256x128x128.)
+  constexpr bool kHelperEnds = CPT == 2 && sizeof(T) == 2;
   // the tcgen05 closure needs all 8 consumer warps busy on every item (two full groups);
   // the host launches it only then, and a lattice where that does not hold steps nothing
   // and reports an error instead of leaving a group barrier short of a warp
@@ -1264,7 +1471,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP, CP
   if (threadIdx.x == 0) {
     for (int s = 0; s < S_; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], n_cons);
+      mbar_init(&empty[s], n_cons + (kHelperEnds ? 1 : 0));
     }
     nan_flag = 0;
     if (!groups_ok) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
@@ -1327,13 +1534,74 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP, CP
 
   if (warp == kHelperWarp) {
     // ---------------- helper warp: this CTA's share of the near-wall cells ----------------
+    // (two cells per thread: and the row-end pairs of every item, one batch of near-wall
+    // cells after each item's pairs)
     const int pslot = (a.step_index + 1) & 1;
     const double corr = a.st->apply[pslot] ? a.st->corr[pslot] : 1.0;
     int my_nan = 0;
-    for (long long t = (long long)blockIdx.x * 32 + lane; t < a.n_near; t += (long long)gridDim.x * 32)
-      my_sum += near_cell<S, MODE, P>(a, a.fsrc, a.fdst, a.write_macro, t, corr,
-                                      [&](int y) { return make_double2(s_uxi[y], s_uyi[y]); }, &my_nan);
+    auto inlet_d = [&](int y) { return make_double2(s_uxi[y], s_uyi[y]); };
+    long long t = (long long)blockIdx.x * 32 + lane;
+    const long long t_step = (long long)gridDim.x * 32;
+    if constexpr (kHelperEnds) {
+      const float corrf = (float)corr;
+      const float2 dec = make_float2(corrf * S::kRawScale, corrf - 1.0f);
+      auto inlet_f = [&](int y) { return make_float2((float)s_uxi[y], (float)s_uyi[y]); };
+      int s = 0;
+      uint32_t ph = 0;
+      long long r0 = item_row0;
+      for (int j = 0; dyn || j < count; ++j, r0 += item_step) {
+        const bool ok = mbar_wait(&full[s], ph, a.wait_limit);
+        if (!__any_sync(0xffffffffu, ok)) {
+          failed = true;
+          break;
+        }
+        if (dyn) {  // the item the producer took for this slot
+          const long long first = s_first[s];
+          if (first < 0) break;
+          r0 = first;
+        }
+        const int nr = (int)(rows - r0 < RYG ? rows - r0 : RYG);
+        for (int e0 = 0; e0 < 2 * nr; e0 += 32) {  // lane e: row e / 2 of the item, end e % 2
+          const int e = e0 + lane;
+          const bool act = e < 2 * nr;
+          const int yy = act ? e >> 1 : 0;
+          const int x0 = act && (e & 1) ? nx - 2 : 0;
+          const T* sp = spop + (size_t)(s * RYG + yy) * 19 * pitch + x0;
+          float2 v[19];
+#pragma unroll
+          for (int d = 0; d < 19; ++d) {
+            const T* q = sp + slot_of(d) * pitch;
+            if (cx_of(d) == 0) v[d] = load_pair<S>(q);
+            else v[d] = make_float2(S::raw(q[-cx_of(d)]), S::raw(q[1 - cx_of(d)]));
+          }
+          const uint32_t cls2 = *reinterpret_cast<const uint16_t*>(scls + (size_t)(s * RYG + yy) * pitch + x0);
+          const int2 yz = s_row[s * RYG + yy];
+          if (e0 + 32 >= 2 * nr) {  // the item's last pull: release the slot
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+          }
+          if (act) {
+            EndGeom g;
+            g.row = r0 + yy; g.nx = nx; g.ny = ny; g.nz = nz; g.pitch = pitch;
+            g.iy = yz.x; g.iz = yz.y; g.x0 = x0;
+            g.wall_row = yz.x == 0 || yz.x == ny - 1 || (nz > 4 && (yz.y == 0 || yz.y == nz - 1));
+            g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro;
+            g.c0 = (uint8_t)(cls2 & 0xffu);
+            g.c1 = (uint8_t)(cls2 >> 8);
+            my_sum += end_pair<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet_f, a, my_nan);
+          }
+        }
+        if (t < a.n_near) {
+          my_sum += near_cell<S, MODE, P>(a, a.fsrc, a.fdst, a.write_macro, t, corr, inlet_d, &my_nan);
+          t += t_step;
+        }
+        if (++s == S_) { s = 0; ph ^= 1u; }
+      }
+    }
+    for (; t < a.n_near; t += t_step)
+      my_sum += near_cell<S, MODE, P>(a, a.fsrc, a.fdst, a.write_macro, t, corr, inlet_d, &my_nan);
     if (__any_sync(0xffffffffu, my_nan) && lane == 0) nan_flag = 1;
+    if (failed && lane == 0) atomicOr(&a.st->error, STEP_ERR_PIPELINE_TIMEOUT);
   } else if (warp == kProducerWarp) {
     // ---------------- producer warp: lanes issue the copies of an item in parallel ----------------
     const uint32_t slot_bytes = (uint32_t)(pitch * sizeof(T));
@@ -1507,7 +1775,8 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE, MLP, CP
             g.wall_row = wall_row; g.ground_no_slip = a.ground_no_slip; g.write_macro = a.write_macro;
             g.c0 = (uint8_t)(cls2 & 0xffu);
             g.c1 = (uint8_t)(cls2 >> 8);
-            pair_segment<S>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a, s_xo + warp * 24, s_dcw,
+            pair_segment<S, decltype(inlet), !kHelperEnds>(v, fd, g, (float)a.tau0, (float)a.k_smag, dec, inlet, a,
+                                                           s_xo + warp * 24, s_dcw,
                             s_dslot, lane, my_sum, my_nan);
           }
         } else
