@@ -5,7 +5,9 @@ arithmetic) and the dynamic deal of work items.
   populations stay within 1e-5 relative of the oracle after 1000 steps (Cd within
   0.5 %), and every storage mode steps like the one-cell-per-thread kernel on awkward
   lattices (one and several chunks per row, nx > 256, short rows, bodies cut by the
-  inlet and outlet planes, ground no-slip).
+  inlet and outlet planes, ground no-slip, a ragged last work item, rows of four cells).
+  With 16-bit storage the pairs that hold a row's ends are the helper warp's (end_pair):
+  the ragged item and the four-cell rows, where the consumers write nothing, test it.
 * The dynamic deal changes only which CTA takes which rows: results are bit-identical
   to the static deal.
 """
@@ -65,6 +67,8 @@ LATTICES = [
     (100, 16, 12, 4.0, 2.0, False),     # body cut by the inlet plane
     (98, 16, 12, 4.0, 96.0, True),      # body cut by the outlet plane, ground no-slip
     (6, 8, 4, 1.0, 3.0, False),         # very short rows, nz <= 4
+    (64, 13, 7, 2.0, 20.0, False),      # a ragged last work item (91 rows, 16-row items at 16 bits)
+    (4, 10, 6, 1.0, 1.5, False),        # every pair of a row holds a row end (nx = 4)
 ]
 
 
