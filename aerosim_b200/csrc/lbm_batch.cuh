@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kStepThreads, step_min_blocks<S, MODE_FAST, ML
       const long long gi = blockIdx.x + (long long)j * gridDim.x;
       const int k = find_instance(b.item_begin, b.n_inst, gi);
       const StepArgs& ia = b.inst[k];
-      const int nx = ia.L.nx, ny = ia.L.ny, nz = ia.L.nz;
+      const int ny = ia.L.ny, nz = ia.L.nz;
       const int pitch = P ? P : ia.L.pitch;
       const int RY = b.geo[k].x;
       const long long rows = (long long)ny * nz;
