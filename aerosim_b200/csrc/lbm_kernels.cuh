@@ -845,36 +845,34 @@ __device__ __forceinline__ long long general_cells(const StepArgs& a, double (&v
 
 // The row ends' equilibria round every operation explicitly (FMA forms), so that the
 // lane-transposed row ends (a run-time direction per lane) and the helper warp's end
-// pairs (end_pair, unrolled directions) give the same bits: w_d ((rho - 1) + rho k) with
-// k = cu + cu^2 / 2 - 1.5 u^2, cu = 3 c_d . u.  The run-time dot product adds the zero
-// products c_a u_a = +-0 that dotc leaves out, which changes no sum but the sign of a
-// zero, and that sign does not reach the result.
-__device__ __forceinline__ float usq_of(float ux, float uy, float uz) {
-  return __fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz)));
+// pairs (end_pair, unrolled directions) give the same bits: in the storage domain
+// OS w_d h + OW w_d with h = A + rho (cu + cu^2 / 2), cu = 3 c_d . u and
+// A = (rho - 1) - 1.5 rho u^2 shared by the cell's directions.  The run-time dot product
+// adds the zero products c_a u_a = +-0 that dotc leaves out, which changes no sum but the
+// sign of a zero, and that sign does not reach the result; OS is a power of two, so OS w_d
+// is exact either way.
+__device__ __forceinline__ float end_A(float rho, float ux, float uy, float uz) {
+  const float usq = __fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz)));
+  return __fmaf_rn(__fmul_rn(-1.5f, rho), usq, __fsub_rn(rho, 1.0f));
 }
-__device__ __forceinline__ float heq_of_dot(float dot, float w, float rho, float usq) {
+template <class S>
+__device__ __forceinline__ float end_eq(float dot, float w, float rho, float A) {
   const float cu = __fmul_rn(3.0f, dot);
-  const float k = __fmaf_rn(-1.5f, usq, __fmaf_rn(__fmul_rn(0.5f, cu), cu, cu));
-  return __fmul_rn(w, __fmaf_rn(rho, k, __fsub_rn(rho, 1.0f)));
+  const float h = __fmaf_rn(rho, __fmaf_rn(__fmul_rn(0.5f, cu), cu, cu), A);
+  return __fmaf_rn(S::kOutScale * w, h, S::kOutW * w);
 }
-// Equilibrium deviation feq - w of a run-time direction c = (c_x, c_y, c_z, w).
-__device__ __forceinline__ float heq_lane(const float4 c, float rho, float ux, float uy, float uz) {
-  const float dot = __fadd_rn(__fadd_rn(__fmul_rn(c.x, ux), __fmul_rn(c.y, uy)), __fmul_rn(c.z, uz));
-  return heq_of_dot(dot, c.w, rho, usq_of(ux, uy, uz));
+// The dot product c . u of a run-time direction c = (c_x, c_y, c_z, w).
+__device__ __forceinline__ float dot_lane(const float4 c, float ux, float uy, float uz) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(c.x, ux), __fmul_rn(c.y, uy)), __fmul_rn(c.z, uz));
 }
 // The row ends' density from their source cell's: 0.85 rho + 0.15 (:336, :358).
 __device__ __forceinline__ float end_rho(float r) { return __fmaf_rn(0.85f, r, 0.15f); }
-// Inlet value in the storage domain from the equilibrium deviation h of weight w (:343-350).
-template <class S>
-__device__ __forceinline__ float inlet_value(float h, float w) {
-  return __fmaf_rn(S::kOutScale, h, S::kOutW * w);
-}
 // Outlet value: 0.75 of the source cell's post-collision value plus 0.25 of the
-// equilibrium of its moments (:361-368).
-template <class S>
-__device__ __forceinline__ float outlet_value(float prev, float h, float w) {
-  return __fmaf_rn(0.75f, prev, __fmul_rn(0.25f, __fmaf_rn(S::kOutScale, h, S::kOutW * w)));
+// equilibrium q of its moments (:361-368), both in the storage domain.
+__device__ __forceinline__ float outlet_blend(float prev, float q) {
+  return __fmaf_rn(0.75f, prev, __fmul_rn(0.25f, q));
 }
+
 // compensate_lanes' correction as lane 0 sums it (the butterfly's order), for a cell whose
 // 19 values one thread holds: the rounding errors of directions 1..18.
 template <class S>
@@ -939,7 +937,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
       float q = 0.0f;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        q = inlet_value<S>(heq_lane(cw, ri, ui.x, ui.y, 0.0f), cw.w);
+        q = end_eq<S>(dot_lane(cw, ui.x, ui.y, 0.0f), cw.w, ri, end_A(ri, ui.x, ui.y, 0.0f));
       }
       q = compensate_lanes<S>(q, lane);
       if (lane < 19) blk[s_dslot[lane] * pitch] = S::store(q);
@@ -977,7 +975,7 @@ __device__ __forceinline__ void fast_segment(float (&v)[19], typename S::T* __re
       if (lane < 19) {
         const float prev = stale ? (float)blk[sl * pitch + nx - 2] : xo[sl];
         const float4 cw = s_dcw[lane];
-        q = outlet_value<S>(prev, heq_lane(cw, ro, mx, my, mz), cw.w);
+        q = outlet_blend(prev, end_eq<S>(dot_lane(cw, mx, my, mz), cw.w, ro, end_A(ro, mx, my, mz)));
       }
       q = compensate_lanes<S>(q, lane);
       if (lane < 19) blk[sl * pitch + nx - 1] = S::store(q);
@@ -1180,7 +1178,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
       float q = 0.0f;
       if (lane < 19) {
         const float4 cw = s_dcw[lane];
-        q = inlet_value<S>(heq_lane(cw, ri, ui.x, ui.y, 0.0f), cw.w);
+        q = end_eq<S>(dot_lane(cw, ui.x, ui.y, 0.0f), cw.w, ri, end_A(ri, ui.x, ui.y, 0.0f));
       }
       q = compensate_lanes<S>(q, lane);
       __syncwarp();  // after lane 0's pair store of cells 0 and 1
@@ -1210,7 +1208,7 @@ __device__ __forceinline__ void pair_segment(float2 (&v)[19], typename S::T* __r
       if (lane < 19) {
         const float prev = stale ? S::raw(blk[sl * pitch + nx - 2]) : xo[sl];
         const float4 cw = s_dcw[lane];
-        q = outlet_value<S>(prev, heq_lane(cw, ro, mx, my, mz), cw.w);
+        q = outlet_blend(prev, end_eq<S>(dot_lane(cw, mx, my, mz), cw.w, ro, end_A(ro, mx, my, mz)));
       }
       q = compensate_lanes<S>(q, lane);
       if (lane < 19) blk[sl * pitch + nx - 1] = S::store(q);
@@ -1279,10 +1277,9 @@ __device__ __forceinline__ long long end_pair(float2 (&v)[19], typename S::T* __
       const float2 ui = inlet_u(g.iy);
       eu = ui.x;
       ev = ui.y;
-      const float us = usq_of(eu, ev, 0.0f);
+      const float A = end_A(er, eu, ev, 0.0f);
 #pragma unroll
-      for (int d = 0; d < 19; ++d)
-        v[d].x = inlet_value<S>(heq_of_dot(dotc(d, eu, ev, 0.0f), wf_of(d), er, us), wf_of(d));
+      for (int d = 0; d < 19; ++d) v[d].x = end_eq<S>(dotc(d, eu, ev, 0.0f), wf_of(d), er, A);
       end = true;
     }
   } else {
@@ -1292,11 +1289,11 @@ __device__ __forceinline__ long long end_pair(float2 (&v)[19], typename S::T* __
       eu = stale ? 0.0f : ux.x;
       ev = stale ? 0.0f : uy.x;
       ew = stale ? 0.0f : uz.x;
-      const float us = usq_of(eu, ev, ew);
+      const float A = end_A(er, eu, ev, ew);
 #pragma unroll
       for (int d = 0; d < 19; ++d) {
         const float prev = stale ? S::raw(out[slot_of(d) * pitch]) : v[d].x;
-        v[d].y = outlet_value<S>(prev, heq_of_dot(dotc(d, eu, ev, ew), wf_of(d), er, us), wf_of(d));
+        v[d].y = outlet_blend(prev, end_eq<S>(dotc(d, eu, ev, ew), wf_of(d), er, A));
       }
       end = true;
     }
